@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""Throughput benchmark: 6-max 100BB MCCFR traversals/s on one or more B200s.
+
+Contract: `python bench.py --gpus N --steps K --warmup W [--impl reference]`
+prints ONE JSON line on rank 0.  A step is one training iteration of the
+workload: N_players player-updates of `batch` traversals each (2^20 for the
+6-max 100BB configuration).  `value` is whole-job traversals/s timed with CUDA
+events on the trainer's stream over exactly K steps, max over ranks; `e2e` is the
+same metric through the C-ABI train call from the host, host<->device copies
+included.  Several GPUs run independent replicas (the trainer keeps one
+device-resident table per GPU, no collective), so scaling is weak.
+
+--impl reference times the reference path's CPU implementation (the C++
+restatement of the reference traversal in oracle/, all host threads) on the
+same workload, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    # name: (preset, overrides, traversals per player-update)
+    "6max-100bb": ("PRESET_6MAX_100BB", {}, 1 << 20),
+    "6max-100bb-refrule": ("PRESET_6MAX_100BB", {"sampling": 0, "max_depth": 64}, 1 << 20),
+    "hu-20bb": ("PRESET_HU_20BB", {}, 1 << 16),
+    "ref8-6max": ("PRESET_REF8", {"num_players": 6, "table_log2": 27}, 1 << 18),
+    "ref8-hu": ("PRESET_REF8", {"table_log2": 27}, 1 << 16),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="6max-100bb")
+    ap.add_argument("--batch", type=int, default=0, help="traversals per player-update (0 = workload default)")
+    ap.add_argument("--no-extras", action="store_true", help="skip the secondary measurements")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_config(L, workload: str, rank: int = 0):
+    preset_name, over, batch = WORKLOADS[workload]
+    cfg = L.preset(getattr(L, preset_name))
+    for k, v in over.items():
+        setattr(cfg, k, v)
+    cfg.seed = int(cfg.seed) + rank  # independent replicas
+    return cfg, batch
+
+
+def describe(cfg, workload, batch) -> dict:
+    kinds = {0: "fold", 1: "check", 2: "call", 3: "check/call", 4: "min-raise", 6: "all-in"}
+    acts = []
+    for a in range(cfg.num_actions):
+        k = cfg.action_kind[a]
+        acts.append(f"{cfg.action_num[a]}/{cfg.action_den[a]}pot" if k == 5 else kinds[k])
+    return {
+        "workload": workload,
+        "players": cfg.num_players,
+        "stack_bb": cfg.starting_stack / cfg.big_blind,
+        "blinds": f"{cfg.small_blind}/{cfg.big_blind} chips",
+        "actions": acts,
+        "raise_cap": cfg.raise_cap,
+        "buckets": [cfg.preflop_buckets, *cfg.postflop_buckets],
+        "sampling": "external" if cfg.sampling == 1 else "reference (outcome at the updating player)",
+        "table_rows": 1 << cfg.table_log2,
+        "key_bits": cfg.key_bits if cfg.key_mode == 1 else 26,
+        "traversals_per_update": batch,
+        "seed": int(cfg.seed),
+        "global_batch": batch * cfg.num_players,
+        "l2": "working set > L2: 130 MB rank table + info-set table of several GB, no flush needed",
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.out = ""
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                self.out = ""
+
+    def summary(self) -> dict:
+        rows = [r for r in csv.reader(io.StringIO(self.out)) if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max((float(r[3]) for r in rows if r[3].strip().replace(".", "").isdigit()),
+                                   default=None)}
+
+
+def measured_peak() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(workload: str) -> dict | None:
+    """DRAM bytes per traversal of the traversal kernel from a committed ncu
+    summary (profiles/traffic.json), if one exists for this workload."""
+    p = ROOT / "profiles" / "traffic.json"
+    try:
+        return json.loads(p.read_text()).get(workload)
+    except Exception:
+        return None
+
+
+def cpu_traversal_rate(L, cfg, batch_sample: int, reps: int = 1) -> tuple[float, dict]:
+    """The oracle (the reference path's C++ restatement) on host cores."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import binding
+
+    threads = os.cpu_count() or 1
+    table = L.hand_table()
+    orc = binding.Oracle(cfg, table)
+    t0 = time.perf_counter()
+    it = 1
+    for r in range(reps):
+        orc.step(it, r % cfg.num_players, batch_sample, threads=threads)
+    dt = time.perf_counter() - t0
+    orc.close()
+    return batch_sample * reps / dt, {"cores": threads, "seconds": dt}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    import __graft_entry__ as ge
+
+    ge.build()
+    m = ge.load_package()
+    L = m.lib
+    cfg, batch = make_config(L, args.workload, rank)
+    if args.batch:
+        batch = args.batch
+    metric = "6-max traversals/s" if cfg.num_players == 6 else "traversals/s"
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        # bounded per-step samples of the same workload on all host cores
+        sample = {"6max-100bb": 1024, "6max-100bb-refrule": 16384, "hu-20bb": 8192}.get(args.workload, 65536)
+        for _ in range(args.warmup):
+            cpu_traversal_rate(L, cfg, max(64, sample // 8))
+        rates, secs = [], 0.0
+        cores = os.cpu_count() or 1
+        for _ in range(args.steps):
+            r, info = cpu_traversal_rate(L, cfg, sample)
+            rates.append(r)
+            secs += info["seconds"]
+            cores = info["cores"]
+        v = statistics.median(rates)
+        desc = f"{sample} traversals of one player-update (iteration 1, player 0) per step, oracle threads={cores}"
+        print(json.dumps({
+            "impl": "reference", "metric": metric, "value": v, "unit": "traversals/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / max(1, args.steps),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": describe(cfg, args.workload, batch),
+            "cpu_baseline": {"value": v, "unit": "traversals/s", "cores": cores, "kind": "port", "sample": desc},
+            "e2e": {"value": v, "unit": "traversals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }), flush=True)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        from datetime import timedelta
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
+    cfg.device = local_rank
+    table = L.hand_table()
+    tr = m.GPUCFRTrainer(config=cfg)
+    tr.set_hand_table(table)
+
+    # warm-up (graph capture happens here)
+    tr.train(args.warmup, batch, verbose=False)
+    s0 = tr.stats()
+    stream = torch.cuda.ExternalStream(tr.stream_ptr(), device=local_rank)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        ev0.record(stream)
+        tr.train(args.steps, batch, verbose=False, timed=True)
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    s1 = tr.stats()
+    ms = ev0.elapsed_time(ev1)
+    trav = s1.traversals - s0.traversals
+    visits = s1.node_visits - s0.node_visits
+    updates = s1.traverser_updates - s0.traverser_updates
+    launches = args.steps * cfg.num_players
+    trav_ms = s1.traverse_ms - s0.traverse_ms
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+        n = torch.tensor([trav], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(n, op=dist.ReduceOp.SUM)
+        total = float(n.item())
+    else:
+        ms_max, total = ms, float(trav)
+    value = total / (ms_max / 1e3)
+
+    # e2e through the C ABI: host call per step, schedule H2D inside, stats D2H read
+    t0 = time.perf_counter()
+    e2e_steps = max(1, args.steps)
+    for _ in range(e2e_steps):
+        tr.train(1, batch, verbose=False)
+        st = tr.stats()
+    e2e_s = time.perf_counter() - t0
+    e2e_local = e2e_steps * batch * cfg.num_players / e2e_s
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_value = world * e2e_steps * batch * cfg.num_players / float(t.item())
+    else:
+        e2e_value = e2e_local
+
+    peak, peak_kind = measured_peak()
+    bytes_per_launch = (40.0 * visits + 96.0 * updates) / launches
+    kernel_ms = trav_ms / launches if trav_ms > 0 else None
+    achieved = bytes_per_launch / (kernel_ms / 1e3) / 1e9 if kernel_ms else None
+    tr_prof = profiled_traffic(args.workload)
+    traffic = None
+    if tr_prof and "dram_bytes_per_traversal" in tr_prof:
+        traffic = tr_prof["dram_bytes_per_traversal"] * (trav / launches)
+
+    out = {
+        "metric": metric, "value": value, "unit": "traversals/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {**describe(cfg, args.workload, batch), "parallelism": f"replicas{world}"},
+        "e2e": {"value": e2e_value, "unit": "traversals/s", "h2d_bytes_per_step": 16,
+                "d2h_bytes_per_step": 44},
+        "gpu_launches": int(args.steps * cfg.num_players * 3),
+        "clocks": clocks.summary(),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "k_traverse_es" if cfg.sampling == 1 else "k_traverse_ref",
+                     "kernel_ms_per_launch": kernel_ms,
+                     "algorithmic_bytes": "40*V + 96*U per launch (V node visits, U updating-player updates)",
+                     "V_per_traversal": visits / max(1, trav), "U_per_traversal": updates / max(1, trav)},
+        "node_visits_per_s": visits / (ms / 1e3) * world,
+    }
+
+    if rank == 0 and world == 1 and not args.no_extras:
+        extras = {}
+        for wl in ("ref8-6max", "6max-100bb-refrule"):
+            if wl == args.workload:
+                continue
+            c2, b2 = make_config(L, wl)
+            t2 = m.GPUCFRTrainer(config=c2)
+            t2.set_hand_table(table)
+            t2.train(3, b2, verbose=False)
+            a0 = t2.stats()
+            st2 = torch.cuda.ExternalStream(t2.stream_ptr(), device=local_rank)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st2)
+            t2.train(5, b2, verbose=False, timed=True)
+            e1.record(st2)
+            e1.synchronize()
+            a1 = t2.stats()
+            ms2 = e0.elapsed_time(e1)
+            n2 = a1.traversals - a0.traversals
+            extras[wl] = {"traversals_per_s": n2 / (ms2 / 1e3), "batch": b2, "iterations": 5,
+                          "traverse_kernel_ms": (a1.traverse_ms - a0.traverse_ms) / (5 * c2.num_players),
+                          "apply_kernel_ms": (a1.apply_ms - a0.apply_ms) / (5 * c2.num_players)}
+            t2.close()
+        out["extras"] = extras
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sample = {"6max-100bb": 2048, "6max-100bb-refrule": 65536, "hu-20bb": 16384}.get(args.workload, 65536)
+        rate, info = cpu_traversal_rate(L, cfg, sample)
+        out["cpu_baseline"] = {"value": rate, "unit": "traversals/s", "cores": info["cores"], "kind": "port",
+                               "sample": f"{sample} traversals of one player-update (iteration 1, player 0), "
+                                         f"{info['seconds']:.1f} s on {info['cores']} threads"}
+    tr.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,240 @@
+/*
+ * mccfr.h — C ABI of the B200 MCCFR trainer (libmccfr.so).
+ *
+ * This is the drop-in boundary for the reference's GPU trainer class
+ * `GPUCFRTrainer` (poker_cuda/src/cfr_gpu.cuh:48-132) and the helpers it calls.
+ * Every entry point returns an int status (MCCFR_OK = 0); nothing in the
+ * library calls exit().  Plain pointers and sizes only: host buffers unless a
+ * parameter name says `dev_`.
+ *
+ * Cards are 0..51 in the reference's suit-major encoding, card = suit*13 + rank
+ * (poker_cuda/src/card.h:8-15), except where a comment says "1..52 codes".
+ */
+#ifndef MCCFR_H
+#define MCCFR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MCCFR_MAX_PLAYERS 6
+#define MCCFR_MAX_ACTIONS 8
+#define MCCFR_HAND_TABLE_ENTRIES 32487834
+#define MCCFR_REF_TABLE_SIZE (1 << 26) /* GPU_TABLE_SIZE, cfr_gpu.cuh:18 */
+
+/* Status codes. */
+enum {
+  MCCFR_OK = 0,
+  MCCFR_ERR_INVALID_ARG = 1,
+  MCCFR_ERR_CUDA = 2,
+  MCCFR_ERR_OOM = 3,
+  MCCFR_ERR_IO = 4,
+  MCCFR_ERR_FORMAT = 5,
+  MCCFR_ERR_NO_HAND_TABLE = 6,
+  MCCFR_ERR_TABLE_FULL = 7,
+  MCCFR_ERR_DEVICE = 8,   /* a kernel raised its error flag (e.g. stack overflow) */
+  MCCFR_ERR_OVERFLOW = 9, /* fixed-point accumulator range would be exceeded */
+  MCCFR_ERR_CAPACITY = 10,/* caller buffer too small; *count holds the size needed */
+  MCCFR_ERR_NO_DEVICE = 11,
+  MCCFR_ERR_TIMEOUT = 12
+};
+
+/* Action slot kinds (the reference's fixed 8 slots are abstraction.h:42-53). */
+enum {
+  MCCFR_ACT_FOLD = 0,
+  MCCFR_ACT_CHECK = 1,
+  MCCFR_ACT_CALL = 2,
+  MCCFR_ACT_CHECK_CALL = 3, /* check when nothing is owed, call otherwise */
+  MCCFR_ACT_RAISE_MIN = 4,
+  MCCFR_ACT_RAISE_POT = 5,  /* raise by num/den of the pot */
+  MCCFR_ACT_ALL_IN = 6
+};
+
+/* Update rule at the updating player's nodes. */
+enum {
+  /* The reference's rule: one action sampled from the BF16 current strategy,
+     importance weight 1/max(strat, 0.05), average strategy accumulated at the
+     updating player's nodes (cfr_gpu.cu:768-838). */
+  MCCFR_SAMPLING_REFERENCE = 0,
+  /* External sampling: every legal action of the updating player is explored;
+     opponents sample one action; the average strategy is accumulated at the
+     sampled opponents' nodes. */
+  MCCFR_SAMPLING_EXTERNAL = 1
+};
+
+/* Info-set identity. */
+enum {
+  MCCFR_KEY_FNV26 = 0, /* the reference's FNV-1a slot & (2^26-1), cfr_gpu.cu:165-179 */
+  MCCFR_KEY_ID64 = 1   /* 64-bit hash of (player, buckets, street, full action path) */
+};
+
+enum { MCCFR_PREFLOP_CHEN64 = 0, MCCFR_PREFLOP_CLASS169 = 1 };
+enum {
+  /* rank-linear buckets on the reference's raw chain values (cfr_gpu.cu:476-489) */
+  MCCFR_POSTFLOP_REF_LINEAR = 0,
+  /* percentile of the true 5/6/7-card rank among all hands of that size */
+  MCCFR_POSTFLOP_RANK_CDF = 1
+};
+
+enum {
+  MCCFR_PRESET_REF8 = 0,       /* the reference's own game and abstraction */
+  MCCFR_PRESET_HU_20BB = 1,    /* heads-up, 20BB, {fold, check/call, pot, all-in}, cap 2 */
+  MCCFR_PRESET_6MAX_100BB = 2  /* 6-max, 100BB, {fold, call, 1/2, pot, 2 pot, all-in}, cap 3 */
+};
+
+typedef struct mccfr_config {
+  int32_t num_players;      /* 2..6 */
+  int32_t starting_stack;   /* chips */
+  int32_t small_blind;
+  int32_t big_blind;
+  int32_t use_cfr_plus;     /* clamp regrets at 0 after each player-update */
+  int32_t use_linear_cfr;   /* average-strategy weight = iteration (else 1) */
+  int32_t sampling;         /* MCCFR_SAMPLING_* */
+  int32_t key_mode;         /* MCCFR_KEY_* */
+  int32_t num_actions;      /* action slots used, 1..8 */
+  int32_t action_kind[MCCFR_MAX_ACTIONS];
+  int32_t action_num[MCCFR_MAX_ACTIONS]; /* pot fraction numerator (RAISE_POT) */
+  int32_t action_den[MCCFR_MAX_ACTIONS]; /* pot fraction denominator (RAISE_POT) */
+  int32_t raise_cap;        /* raises per street; 0 = unlimited (the reference) */
+  int32_t max_depth;        /* depth cut; the reference returns 0 at depth 20 */
+  int32_t preflop_mode;     /* MCCFR_PREFLOP_* */
+  int32_t preflop_buckets;  /* 64 for CHEN64, 169 for CLASS169 */
+  int32_t postflop_mode;    /* MCCFR_POSTFLOP_* */
+  int32_t postflop_buckets[3]; /* flop, turn, river */
+  int32_t table_log2;       /* info-set table capacity = 2^table_log2 rows */
+  int32_t device;           /* CUDA device ordinal */
+  uint64_t seed;            /* Philox key */
+  /* ID64 keys only: when > 0, keys are reduced to key_bits bits (plus one), so
+     at most 2^key_bits rows exist and identities that share the reduced key share
+     a row, as the reference's 2^26 direct-mapped slots do.  0 = full 64 bits. */
+  int32_t key_bits;
+  int32_t reserved[7];
+} mccfr_config;
+
+/* Counters and timings of one handle. */
+typedef struct mccfr_stats {
+  int64_t iterations_done;   /* completed iterations t */
+  int64_t launches;          /* player-updates launched */
+  int64_t traversals;
+  int64_t node_visits;       /* decision nodes visited (V) */
+  int64_t traverser_updates; /* updating-player nodes updated (U) */
+  int64_t terminals;         /* terminal values computed */
+  int64_t hand_evals;        /* rank-chain evaluations */
+  int64_t rows_used;         /* occupied info-set rows */
+  int64_t table_capacity;
+  int64_t touched_last;      /* rows touched by the last player-update */
+  double traverse_ms;        /* summed CUDA-event time of traversal kernels */
+  double apply_ms;           /* summed CUDA-event time of apply kernels */
+  double last_traverse_ms;
+  double last_apply_ms;
+  int32_t device_error;      /* sticky kernel error bits */
+  int32_t reserved[7];
+} mccfr_stats;
+
+/* One traversal's record from mccfr_step_trace (reference sampling mode). */
+typedef struct mccfr_trace {
+  uint8_t hole[12];           /* [player*2 + i] */
+  uint8_t board[5];
+  uint8_t dealer;
+  uint8_t n_actions;          /* actions taken along the sampled path */
+  uint8_t n_traverser_nodes;
+  uint8_t hole_bucket[6];
+  uint8_t board_bucket[6][4]; /* [player][street] */
+  uint8_t actions[40];        /* action slots, in order */
+  float payoff;               /* terminal value for the updating player */
+  uint32_t reserved;
+} mccfr_trace;
+
+typedef struct mccfr_handle mccfr_handle;
+
+/* ---- configuration ---------------------------------------------------- */
+/* Fills *cfg with a preset; the REF8 preset reproduces the constructor defaults of
+   GPUCFRTrainer (cfr_gpu.cuh:50-55): 2 players, stack 1000, blinds 10/20, CFR+ and
+   linear CFR on, the 8 fixed action slots, 64 Chen buckets, 128 rank buckets. */
+int mccfr_config_init(mccfr_config* cfg, int preset);
+
+/* ---- lifetime (replaces GPUCFRTrainer::GPUCFRTrainer / ~GPUCFRTrainer,
+        cfr_gpu.cu:1064-1084) ------------------------------------------- */
+int mccfr_create(const mccfr_config* cfg, mccfr_handle** out);
+void mccfr_destroy(mccfr_handle* h);
+
+/* ---- hand-rank table (replaces GPUCFRTrainer::load_hand_table,
+        cfr_gpu.cu:1086-1104, and hand_eval_init, hand_eval.cpp:88-102) -- */
+/* Reads a 32,487,834-entry int32 file and validates it like the reference
+   (size + As Ks Qs Js Ts 2c 3d decodes to 7462). */
+int mccfr_load_hand_table(mccfr_handle* h, const char* path);
+/* Uploads a table already in host memory (n must be MCCFR_HAND_TABLE_ENTRIES). */
+int mccfr_set_hand_table(mccfr_handle* h, const int32_t* table, size_t n);
+/* Builds the table on the host (no reference counterpart: the reference's
+   generator, tools/gen_lookup_table.cpp:63-97, is a stub). */
+int mccfr_hand_table_generate(int32_t* out, size_t n);
+int mccfr_hand_table_write(const char* path);
+int mccfr_hand_class_count(void);
+
+/* ---- training (replaces GPUCFRTrainer::train, cfr_gpu.cu:1244-1378) --- */
+/* Runs `iters` iterations; each iteration is one player-update of `batch`
+   traversals per player.  Checkpoints to ckpt_path every ckpt_interval
+   iterations when ckpt_path is non-empty. */
+int mccfr_train(mccfr_handle* h, long long iters, int batch, int verbose,
+                const char* ckpt_path, long long ckpt_interval);
+/* One player-update (iteration t >= 1, player p) of `batch` traversals.  When
+   trace != NULL (reference sampling only), one record per traversal is copied
+   to trace[0..batch). */
+int mccfr_step(mccfr_handle* h, long long iteration, int player, int batch,
+               mccfr_trace* trace);
+
+/* ---- results (replaces get_strategy / num_info_sets_active /
+        export_tables / import_tables, cfr_gpu.cu:1383-1459) ------------- */
+/* Normalised average strategy, one row per info-set key with a non-zero sum,
+   sorted by key.  keys[i] is the reference's u32 dump key (the FNV slot) in
+   FNV26 mode and the low 32 bits of the 64-bit key otherwise; keys64 (optional)
+   receives full keys.  probs is [capacity][8]. */
+int mccfr_get_strategy(mccfr_handle* h, uint32_t* keys, uint64_t* keys64,
+                       float* probs, size_t capacity, size_t* count);
+int mccfr_num_info_sets_active(mccfr_handle* h, long long* out);
+/* Every occupied row, sorted by key: regrets [8], strategy sums [8] and the
+   number of updates the row received. */
+int mccfr_export_rows(mccfr_handle* h, uint64_t* keys, float* regrets,
+                      float* strategy_sum, uint64_t* visits, size_t capacity,
+                      size_t* count);
+/* Dense SoA [8][2^26] tables of the reference (FNV26 mode only). */
+int mccfr_export_tables(mccfr_handle* h, float* regrets, float* strategy_sum,
+                        size_t n);
+int mccfr_import_tables(mccfr_handle* h, const float* regrets,
+                        const float* strategy_sum, size_t n);
+
+/* ---- files (replaces save/load_checkpoint, cfr_gpu.cu:1464-1538, and
+        strategy_save, strategy.cpp:35-52) ------------------------------ */
+/* Checkpoint in the reference's layout: [u64 0x43465247505500][u32 2^26]
+   [u32 8] regrets[8][2^26] strategy_sum[8][2^26] (FNV26 mode only). */
+int mccfr_save_checkpoint(mccfr_handle* h, const char* path);
+int mccfr_load_checkpoint(mccfr_handle* h, const char* path);
+/* Strategy dump v2: [u64 0x53545241540100][u32 2^26][u32 8][u32 n]{u32 key, f32[8]}. */
+int mccfr_save_strategy(mccfr_handle* h, const char* path);
+
+/* ---- introspection ----------------------------------------------------- */
+int mccfr_get_stats(mccfr_handle* h, mccfr_stats* out);
+int mccfr_get_config(mccfr_handle* h, mccfr_config* out);
+const char* mccfr_strerror(int status);
+/* sizeof(mccfr_config), sizeof(mccfr_stats), sizeof(mccfr_trace), for bindings. */
+int mccfr_abi_sizes(size_t* out3);
+/* The cudaStream_t (as void*) every kernel of the handle is launched on. */
+int mccfr_get_stream(mccfr_handle* h, void** stream);
+const char* mccfr_last_error(mccfr_handle* h);
+
+/* ---- showdown evaluation (hand-eval microbenchmark) ----------------------- */
+/* ranks[i] = 7-card rank (1..7462) of cards[7*i .. 7*i+6] for i < n, computed on
+   the device with the handle's table. */
+int mccfr_eval7(mccfr_handle* h, const uint8_t* cards, uint16_t* ranks, size_t n);
+/* Same on device buffers (dev_cards, dev_ranks), on the handle's stream; the
+   call returns after the kernel finished; *ms receives its CUDA-event time. */
+int mccfr_eval7_device(mccfr_handle* h, const uint8_t* dev_cards,
+                       uint16_t* dev_ranks, size_t n, float* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MCCFR_H */

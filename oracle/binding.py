@@ -1,0 +1,184 @@
+"""ctypes binding of the oracle (liboracle.so) and of the reference shim (_ref/libref.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg, as the checker.  The product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_char_p, c_float, c_int, c_int64, c_longlong, c_size_t, c_uint32, c_void_p
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_LIB = HERE / "liboracle.so"
+REF_LIB = HERE / "_ref" / "libref.so"
+
+
+def _p(a: np.ndarray) -> c_void_p:
+    return c_void_p(a.ctypes.data)
+
+
+_orc = None
+
+
+def lib() -> ctypes.CDLL:
+    global _orc
+    if _orc is None:
+        if not ORACLE_LIB.exists():
+            raise RuntimeError(f"{ORACLE_LIB} missing: run `make -C oracle`")
+        o = ctypes.CDLL(str(ORACLE_LIB))
+        o.orc_create.restype = c_void_p
+        o.orc_create.argtypes = [c_void_p, c_void_p]
+        o.orc_destroy.argtypes = [c_void_p]
+        o.orc_set_float_mode.argtypes = [c_void_p, c_int]
+        o.orc_step.argtypes = [c_void_p, c_longlong, c_int, c_int, c_void_p, c_int]
+        o.orc_train.argtypes = [c_void_p, c_longlong, c_int, c_int]
+        o.orc_counters.argtypes = [c_void_p, c_void_p]
+        o.orc_export_rows.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, POINTER(c_size_t)]
+        o.orc_get_strategy.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, POINTER(c_size_t)]
+        o.orc_philox.argtypes = [c_void_p, c_void_p, c_void_p]
+        o.orc_uniform01.restype = c_float
+        o.orc_uniform01.argtypes = [c_uint32]
+        o.orc_eval7.argtypes = [c_void_p, c_void_p, c_void_p, c_size_t]
+        o.orc_ref_board_bucket.argtypes = [c_void_p, c_int, c_int, c_void_p, c_int, c_int]
+        o.orc_preflop_lut.argtypes = [c_int, c_int, c_void_p]
+        o.orc_rank_cdf_lut.argtypes = [c_void_p, c_int, c_int, c_void_p]
+        o.orc_rank_hist.argtypes = [c_void_p, c_int, c_void_p]
+        o.orc_chain_rank.argtypes = [c_void_p, c_void_p, c_int]
+        o.orc_valid_mask.argtypes = [c_void_p, c_int, c_int, c_int, c_int, c_int, c_int]
+        o.orc_chips.argtypes = [c_void_p, c_int, c_int, c_int, c_int, c_int, c_int]
+        o.orc_regret_frac_bits.argtypes = [c_void_p, c_longlong]
+        o.brute_rank.argtypes = [c_void_p, c_int]
+        o.brute_rank_batch.argtypes = [c_void_p, c_int, c_void_p, c_size_t, c_int]
+        _orc = o
+    return _orc
+
+
+class Oracle:
+    """CPU restatement of one trainer (same config struct as the product)."""
+
+    def __init__(self, config, hand_table: np.ndarray):
+        self._t = np.ascontiguousarray(hand_table, dtype=np.int32)  # kept alive (borrowed by C)
+        self._cfg = config
+        self._h = lib().orc_create(ctypes.byref(config), _p(self._t))
+
+    def close(self):
+        if self._h:
+            lib().orc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_float_mode(self, on: bool):
+        lib().orc_set_float_mode(self._h, 1 if on else 0)
+
+    def step(self, iteration: int, player: int, batch: int, trace: bool = False, threads: int = 8,
+             trace_dtype=None):
+        buf = np.zeros(batch, dtype=trace_dtype) if trace else None
+        lib().orc_step(self._h, iteration, player, batch, _p(buf) if trace else None, threads)
+        return buf
+
+    def train(self, iters: int, batch: int, threads: int = 8):
+        lib().orc_train(self._h, iters, batch, threads)
+
+    def counters(self) -> dict:
+        c = np.zeros(6, dtype=np.int64)
+        lib().orc_counters(self._h, _p(c))
+        return dict(zip(["traversals", "visits", "updates", "evals", "terminals", "rows"], c.tolist()))
+
+    def export_rows(self) -> dict:
+        n = c_size_t()
+        lib().orc_export_rows(self._h, None, None, None, None, 0, ctypes.byref(n))
+        m = n.value
+        keys = np.empty(m, np.uint64)
+        reg = np.empty((m, 8), np.float32)
+        ssum = np.empty((m, 8), np.float32)
+        vis = np.empty(m, np.uint64)
+        lib().orc_export_rows(self._h, _p(keys), _p(reg), _p(ssum), _p(vis), m, ctypes.byref(n))
+        return {"keys": keys, "regrets": reg, "strategy_sum": ssum, "visits": vis}
+
+    def strategy_arrays(self):
+        n = c_size_t()
+        lib().orc_get_strategy(self._h, None, None, None, 0, ctypes.byref(n))
+        m = n.value
+        keys = np.empty(m, np.uint32)
+        probs = np.empty((m, 8), np.float32)
+        lib().orc_get_strategy(self._h, _p(keys), None, _p(probs), m, ctypes.byref(n))
+        return keys[: n.value], probs[: n.value]
+
+
+def philox(ctr, key) -> np.ndarray:
+    c = np.asarray(ctr, dtype=np.uint32)
+    k = np.asarray(key, dtype=np.uint32)
+    out = np.zeros(4, dtype=np.uint32)
+    lib().orc_philox(_p(c), _p(k), _p(out))
+    return out
+
+
+def eval7(table: np.ndarray, cards: np.ndarray) -> np.ndarray:
+    c = np.ascontiguousarray(cards, dtype=np.uint8).reshape(-1, 7)
+    out = np.empty(c.shape[0], dtype=np.uint16)
+    lib().orc_eval7(_p(table), _p(c), _p(out), c.shape[0])
+    return out
+
+
+def brute_ranks(cards: np.ndarray, n: int, threads: int = 8) -> np.ndarray:
+    c = np.ascontiguousarray(cards, dtype=np.uint8).reshape(-1, n)
+    out = np.empty(c.shape[0], dtype=np.uint16)
+    lib().brute_rank_batch(_p(c), n, _p(out), c.shape[0], threads)
+    return out
+
+
+def rank_hist(table: np.ndarray, ncards: int) -> np.ndarray:
+    out = np.zeros(7463, dtype=np.uint64)
+    lib().orc_rank_hist(_p(table), ncards, _p(out))
+    return out
+
+
+def preflop_lut(mode: int, buckets: int) -> np.ndarray:
+    out = np.zeros(52 * 52, dtype=np.uint8)
+    lib().orc_preflop_lut(mode, buckets, _p(out))
+    return out
+
+
+def chain_rank(table: np.ndarray, cards) -> int:
+    c = np.ascontiguousarray(cards, dtype=np.uint8)
+    return lib().orc_chain_rank(_p(table), _p(c), c.size)
+
+
+def valid_mask(cfg, pot, stack, to_call, cb, lfr, raises=0) -> int:
+    return lib().orc_valid_mask(ctypes.byref(cfg), pot, stack, to_call, cb, lfr, raises)
+
+
+def chips(cfg, a, pot, stack, to_call, cb, lfr) -> int:
+    return lib().orc_chips(ctypes.byref(cfg), a, pot, stack, to_call, cb, lfr)
+
+
+# ---- the reference's own CPU functions (compiled from its sources) -----------
+_ref = None
+
+
+def ref_available() -> bool:
+    return REF_LIB.exists()
+
+
+def ref() -> ctypes.CDLL:
+    global _ref
+    if _ref is None:
+        r = ctypes.CDLL(str(REF_LIB))
+        r.ref_hand_eval_init.argtypes = [c_char_p]
+        r.ref_evaluate_7cards.argtypes = [c_void_p]
+        r.ref_evaluate_best.argtypes = [c_int, c_int, c_void_p, c_int]
+        r.ref_preflop_bucket.argtypes = [c_int, c_int]
+        r.ref_fast_postflop_bucket.argtypes = [c_int, c_int, c_void_p, c_int]
+        r.ref_valid_actions_mask.argtypes = [c_int] * 6
+        r.ref_action_to_chips.argtypes = [c_int] * 7
+        r.ref_abstraction_init()
+        _ref = r
+    return _ref

@@ -1,0 +1,1179 @@
+// mccfr.cu — kernels and C ABI of the B200 MCCFR trainer (see include/mccfr.h).
+//
+// Host side of the reference's GPUCFRTrainer (poker_cuda/src/cfr_gpu.cu:1064-1538)
+// restructured for one device-resident table:
+//   * the dense regret-matching and clamp sweeps of every player-update
+//     (cfr_gpu.cu:318-351, 1018-1022) are replaced by computing the current
+//     strategy in the traversal from the row it reads, plus an apply kernel that
+//     visits only the rows the update touched;
+//   * one iteration (N player-updates x [traverse, apply, advance]) is captured
+//     once as a CUDA graph and replayed; the iteration and player are advanced on
+//     the device, so replays need no host copies (cfr_gpu.cu:1303-1322 copies
+//     two scalars per update);
+//   * errors are returned as status codes, never exit() (cfr_gpu.cu:61-69).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mccfr.h"
+#include "game.cuh"
+#include "handtable.h"
+#include "table.cuh"
+#include "traverse_ref.cuh"
+#include "traverse_es.cuh"
+
+namespace mccfr {
+void build_preflop_lut(int mode, int buckets, uint8_t* lut);
+void build_cdf_lut(const unsigned long long* counts, int buckets, uint8_t* lut);
+}  // namespace mccfr
+
+using namespace mccfr;
+
+// ---------------------------------------------------------------------------
+// Small kernels
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kRefBlock = 128;
+
+__global__ void k_advance(Sched* s, int N) {
+  int p = s->player + 1;
+  if (p >= N) {
+    p = 0;
+    s->iteration += 1;
+  }
+  s->player = p;
+}
+
+// Folds one player-update's accumulators into the rows it touched and zeroes
+// them (the sparse equivalent of kernel_clamp_regrets, cfr_gpu.cu:1018-1022).
+__global__ void __launch_bounds__(256) k_apply(const GameParams G, const TableView tv,
+                                               const Sched* __restrict__ sched, double rinv) {
+  const long long iteration = sched->iteration;
+  const uint32_t uid = (uint32_t)((iteration - 1) * G.N + sched->player);
+  const unsigned n = tv.n_touched[uid & 1];
+  const double w = G.lcfr ? (double)(float)iteration : 1.0;
+  const double s32 = 2.3283064365386962890625e-10;  // 2^-32
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned long long slot = tv.touched[i];
+    const uint32_t m = (uint32_t)(tv.tag[slot] & 0xFF);
+    const unsigned long long cnt = tv.cnt[slot];
+    const long long canon = (long long)(cnt & 0xFFFFFFFFull);
+    const long long su = tv.su[slot];
+    const float4 r0 = tv.reg[2 * slot], r1 = tv.reg[2 * slot + 1];
+    const float4 q0 = tv.ssum[2 * slot], q1 = tv.ssum[2 * slot + 1];
+    float reg[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
+    float ss[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+    float strat[8];
+    node_strategy(reg, m, strat);
+    long long* da = tv.da + 8 * slot;
+    long long* ds = tv.ds + 8 * slot;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const bool in = (m >> a) & 1;
+      const long long dr = da[a] - (in ? su : 0ll);
+      const long long dsv = ds[a] + (in ? canon * fix_s(strat[a]) : 0ll);
+      float r = __fadd_rn(reg[a], __double2float_rn(__dmul_rn((double)dr, rinv)));
+      if (G.cfr_plus) r = (r < 0.0f) ? 0.0f : r;
+      reg[a] = r;
+      ss[a] = __fadd_rn(ss[a], __double2float_rn(__dmul_rn(__dmul_rn((double)dsv, s32), w)));
+      da[a] = 0;
+      ds[a] = 0;
+    }
+    tv.reg[2 * slot] = make_float4(reg[0], reg[1], reg[2], reg[3]);
+    tv.reg[2 * slot + 1] = make_float4(reg[4], reg[5], reg[6], reg[7]);
+    tv.ssum[2 * slot] = make_float4(ss[0], ss[1], ss[2], ss[3]);
+    tv.ssum[2 * slot + 1] = make_float4(ss[4], ss[5], ss[6], ss[7]);
+    tv.visits[slot] += cnt >> 32;
+    tv.cnt[slot] = 0;
+    tv.su[slot] = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) tv.n_touched[(uid + 1) & 1] = 0;
+}
+
+__global__ void k_export(const TableView tv, unsigned long long cap_slots,
+                         unsigned long long* __restrict__ okeys, float4* __restrict__ oreg,
+                         float4* __restrict__ ossum, unsigned long long* __restrict__ ovis,
+                         unsigned int* __restrict__ on) {
+  for (unsigned long long s = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; s < cap_slots;
+       s += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long k = tv.keys[s];
+    if (!k) continue;
+    const unsigned i = atomicAdd(on, 1u);
+    okeys[i] = k;
+    oreg[2 * i] = tv.reg[2 * s];
+    oreg[2 * i + 1] = tv.reg[2 * s + 1];
+    ossum[2 * i] = tv.ssum[2 * s];
+    ossum[2 * i + 1] = tv.ssum[2 * s + 1];
+    ovis[i] = tv.visits[s];
+  }
+}
+
+// Inserts dense reference-layout rows (FNV slot + 1 as key) with any non-zero
+// value (load_checkpoint / import_tables).
+__global__ void k_import_dense(const TableView tv, const float* __restrict__ dr, const float* __restrict__ ds,
+                               unsigned n_slots) {
+  for (unsigned s = blockIdx.x * blockDim.x + threadIdx.x; s < n_slots; s += gridDim.x * blockDim.x) {
+    float r[8], q[8];
+    bool any = false;
+    for (int a = 0; a < 8; ++a) {
+      r[a] = dr[(size_t)a * n_slots + s];
+      q[a] = ds[(size_t)a * n_slots + s];
+      any |= (r[a] != 0.0f) || (q[a] != 0.0f);
+    }
+    if (!any) continue;
+    const long long slot = table_insert(tv, (unsigned long long)s + 1);
+    if (slot < 0) continue;
+    tv.reg[2 * slot] = make_float4(r[0], r[1], r[2], r[3]);
+    tv.reg[2 * slot + 1] = make_float4(r[4], r[5], r[6], r[7]);
+    tv.ssum[2 * slot] = make_float4(q[0], q[1], q[2], q[3]);
+    tv.ssum[2 * slot + 1] = make_float4(q[4], q[5], q[6], q[7]);
+  }
+}
+
+__global__ void k_export_dense(const TableView tv, unsigned long long cap_slots, float* __restrict__ dr,
+                               float* __restrict__ ds, unsigned n_slots) {
+  for (unsigned long long s = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; s < cap_slots;
+       s += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long k = tv.keys[s];
+    if (!k || k > n_slots) continue;
+    const unsigned d = (unsigned)(k - 1);
+    const float* r = reinterpret_cast<const float*>(tv.reg + 2 * s);
+    const float* q = reinterpret_cast<const float*>(tv.ssum + 2 * s);
+    for (int a = 0; a < 8; ++a) {
+      dr[(size_t)a * n_slots + d] = r[a];
+      ds[(size_t)a * n_slots + d] = q[a];
+    }
+  }
+}
+
+// CFR+ clamp of every row (after importing regrets that may be negative).
+__global__ void k_clamp_all(const TableView tv, unsigned long long cap_slots) {
+  for (unsigned long long s = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; s < cap_slots;
+       s += (unsigned long long)gridDim.x * blockDim.x) {
+    float4 a = tv.reg[2 * s], b = tv.reg[2 * s + 1];
+    a.x = a.x < 0.f ? 0.f : a.x; a.y = a.y < 0.f ? 0.f : a.y; a.z = a.z < 0.f ? 0.f : a.z; a.w = a.w < 0.f ? 0.f : a.w;
+    b.x = b.x < 0.f ? 0.f : b.x; b.y = b.y < 0.f ? 0.f : b.y; b.z = b.z < 0.f ? 0.f : b.z; b.w = b.w < 0.f ? 0.f : b.w;
+    tv.reg[2 * s] = a;
+    tv.reg[2 * s + 1] = b;
+  }
+}
+
+// One thread per 7-card hand: 7 dependent gathers (hand_eval.cpp:134-143).
+__global__ void k_eval7(const int32_t* __restrict__ T, const uint8_t* __restrict__ cards,
+                        uint16_t* __restrict__ ranks, unsigned long long n) {
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const uint8_t* c = cards + 7 * i;
+    int32_t p = __ldg(T + 53 + to_rm(c[0]));
+#pragma unroll
+    for (int k = 1; k < 7; ++k) p = __ldg(T + p + to_rm(c[k]));
+    ranks[i] = (uint16_t)decode16((uint32_t)p & 0xFFFF);
+  }
+}
+
+// Exact rank histogram of all C(52, n) hands (n = 5, 6, 7), one thread per
+// ordered 3-card prefix a<b<c.
+__global__ void k_rank_hist(const int32_t* __restrict__ T, int ncards, unsigned long long* __restrict__ hist) {
+  __shared__ unsigned int sh[7463];
+  for (int i = threadIdx.x; i < 7463; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
+  const unsigned id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id < 52u * 52u * 52u) {
+    const int a = id / 2704, b = (id / 52) % 52, c = id % 52;
+    if (a < b && b < c) {
+      const int32_t pc = __ldg(T + __ldg(T + __ldg(T + 53 + to_rm(a)) + to_rm(b)) + to_rm(c));
+      for (int d = c + 1; d < 52; ++d) {
+        const int32_t pd = __ldg(T + pc + to_rm(d));
+        for (int e = d + 1; e < 52; ++e) {
+          const int32_t pe = __ldg(T + pd + to_rm(e));
+          if (ncards == 5) {
+            atomicAdd(&sh[decode16((uint32_t)__ldg(T + pe) & 0xFFFF)], 1u);
+            continue;
+          }
+          for (int f = e + 1; f < 52; ++f) {
+            const int32_t pf = __ldg(T + pe + to_rm(f));
+            if (ncards == 6) {
+              atomicAdd(&sh[decode16((uint32_t)__ldg(T + pf) & 0xFFFF)], 1u);
+              continue;
+            }
+            for (int g = f + 1; g < 52; ++g)
+              atomicAdd(&sh[decode16((uint32_t)__ldg(T + pf + to_rm(g)) & 0xFFFF)], 1u);
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 7463; i += blockDim.x)
+    if (sh[i]) atomicAdd(&hist[i], (unsigned long long)sh[i]);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Handle
+// ---------------------------------------------------------------------------
+struct mccfr_handle {
+  mccfr_config cfg;
+  GameParams gp;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t gev[3 * MCCFR_MAX_PLAYERS] = {};  // per update in the graph: start, after traverse, after apply
+  // hand data
+  int32_t* d_hr = nullptr;
+  uint8_t* d_pre = nullptr;
+  uint8_t* d_cdf = nullptr;
+  bool has_table = false;
+  // info-set table
+  unsigned long long cap = 0;
+  TableView tv{};
+  void* d_block = nullptr;  // one allocation for the table arrays
+  Sched* d_sched = nullptr;
+  Sched* h_sched = nullptr;  // pinned
+  Counters* d_counters = nullptr;
+  // graph of one iteration
+  cudaGraphExec_t graph = nullptr;
+  int graph_batch = -1;
+  long long iterations_done = 0;
+  long long launches = 0;
+  double traverse_ms = 0, apply_ms = 0, last_traverse_ms = 0, last_apply_ms = 0;
+  long long touched_last = 0;
+  int sticky_err = 0;
+  std::string last_error;
+  size_t persist_prev = 0;
+  bool persist_set = false;
+};
+
+namespace {
+
+int fail(mccfr_handle* h, int code, const char* fmt, ...) {
+  if (h) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    h->last_error = buf;
+  }
+  return code;
+}
+
+#define CK(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess)                                                                    \
+      return fail(h, e_ == cudaErrorMemoryAllocation ? MCCFR_ERR_OOM : MCCFR_ERR_CUDA,        \
+                  "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+int regret_frac_bits(const mccfr_config& c, long long batch) {
+  auto bitlen = [](unsigned long long v) {
+    int b = 0;
+    while (v) {
+      ++b;
+      v >>= 1;
+    }
+    return b;
+  };
+  const unsigned long long span =
+      20ull * (unsigned long long)c.num_players * (unsigned long long)std::max(1, c.starting_stack);
+  int rb = 61 - bitlen((unsigned long long)batch) - bitlen(span) - 6;
+  return std::min(24, std::max(8, rb));
+}
+
+int validate(const mccfr_config& c, std::string& why) {
+  if (c.num_players < 2 || c.num_players > 6) return why = "num_players must be 2..6", 1;
+  if (c.starting_stack <= 0 || c.starting_stack > 65535) return why = "starting_stack must be 1..65535", 1;
+  if (c.small_blind < 0 || c.big_blind <= 0 || c.small_blind > c.starting_stack || c.big_blind > c.starting_stack)
+    return why = "blinds must be positive and at most the stack", 1;
+  if (c.num_actions < 1 || c.num_actions > 8) return why = "num_actions must be 1..8", 1;
+  bool has_fold = false, has_check = false;
+  for (int a = 0; a < c.num_actions; ++a) {
+    const int k = c.action_kind[a];
+    if (k < 0 || k > 6) return why = "unknown action kind", 1;
+    if (k == MCCFR_ACT_RAISE_POT && (c.action_den[a] <= 0 || c.action_num[a] <= 0 || c.action_num[a] > 16))
+      return why = "RAISE_POT needs 0 < num <= 16 and den > 0", 1;
+    has_fold |= k == MCCFR_ACT_FOLD;
+    has_check |= k == MCCFR_ACT_CHECK || k == MCCFR_ACT_CHECK_CALL;
+  }
+  if (!has_fold || !has_check) return why = "action set needs a fold slot and a check (or check/call) slot", 1;
+  if (c.sampling != MCCFR_SAMPLING_REFERENCE && c.sampling != MCCFR_SAMPLING_EXTERNAL)
+    return why = "unknown sampling mode", 1;
+  if (c.key_mode != MCCFR_KEY_FNV26 && c.key_mode != MCCFR_KEY_ID64) return why = "unknown key mode", 1;
+  if (c.max_depth < 1 || c.max_depth > 255) return why = "max_depth must be 1..255", 1;
+  if (c.raise_cap < 0 || c.raise_cap > 15) return why = "raise_cap must be 0..15", 1;
+  if (c.preflop_mode == MCCFR_PREFLOP_CHEN64) {
+    if (c.preflop_buckets < 1 || c.preflop_buckets > 256) return why = "preflop_buckets must be 1..256", 1;
+  } else if (c.preflop_mode == MCCFR_PREFLOP_CLASS169) {
+    if (c.preflop_buckets != 169) return why = "CLASS169 needs preflop_buckets = 169", 1;
+  } else {
+    return why = "unknown preflop mode", 1;
+  }
+  if (c.postflop_mode != MCCFR_POSTFLOP_REF_LINEAR && c.postflop_mode != MCCFR_POSTFLOP_RANK_CDF)
+    return why = "unknown postflop mode", 1;
+  for (int s = 0; s < 3; ++s)
+    if (c.postflop_buckets[s] < 1 || c.postflop_buckets[s] > 256) return why = "postflop buckets must be 1..256", 1;
+  if (c.table_log2 < 10 || c.table_log2 > 31) return why = "table_log2 must be 10..31", 1;
+  if (c.key_bits < 0 || c.key_bits > 48) return why = "key_bits must be 0..48", 1;
+  // Reference rule walks one path; its records hold the updating player's nodes.
+  if (c.sampling == MCCFR_SAMPLING_REFERENCE && c.raise_cap == 0 && c.max_depth > 2 * kMaxRec)
+    return why = "reference sampling without a raise cap needs max_depth <= 64", 1;
+  return 0;
+}
+
+void make_params(const mccfr_config& c, GameParams& g) {
+  std::memset(&g, 0, sizeof(g));
+  g.N = c.num_players;
+  g.stack = c.starting_stack;
+  g.sb = c.small_blind;
+  g.bb = c.big_blind;
+  g.cfr_plus = c.use_cfr_plus;
+  g.lcfr = c.use_linear_cfr;
+  g.sampling = c.sampling;
+  g.key_mode = c.key_mode;
+  g.num_actions = c.num_actions;
+  g.raise_cap = c.raise_cap;
+  g.max_depth = c.max_depth;
+  g.postflop_mode = c.postflop_mode;
+  for (int s = 0; s < 3; ++s) g.post_b[s] = c.postflop_buckets[s];
+  g.seed_lo = (uint32_t)c.seed;
+  g.seed_hi = (uint32_t)(c.seed >> 32);
+  g.key_bits = c.key_mode == MCCFR_KEY_ID64 ? c.key_bits : 0;
+  for (int a = 0; a < 8; ++a) {
+    g.kind[a] = (int8_t)(a < c.num_actions ? c.action_kind[a] : -1);
+    g.num[a] = (int16_t)(a < c.num_actions ? c.action_num[a] : 0);
+    g.den[a] = (int16_t)(a < c.num_actions ? std::max(1, c.action_den[a]) : 1);
+    const int k = g.kind[a];
+    if (k == MCCFR_ACT_FOLD) g.m_fold |= 1u << a;
+    if (k == MCCFR_ACT_CHECK || k == MCCFR_ACT_CHECK_CALL) g.m_check |= 1u << a;
+    if (k == MCCFR_ACT_CALL || k == MCCFR_ACT_CHECK_CALL) g.m_call |= 1u << a;
+    if (k == MCCFR_ACT_ALL_IN) g.m_allin |= 1u << a;
+    if (k == MCCFR_ACT_RAISE_MIN || k == MCCFR_ACT_RAISE_POT) g.m_raise |= 1u << a;
+  }
+  // Passive fallback order (cfr_gpu.cu:498-508): check, check/call, call, fold,
+  // raises in slot order, all-in.
+  const int order[] = {MCCFR_ACT_CHECK, MCCFR_ACT_CHECK_CALL, MCCFR_ACT_CALL, MCCFR_ACT_FOLD, -2,
+                       MCCFR_ACT_ALL_IN};
+  g.n_fallback = 0;
+  for (int k : order)
+    for (int a = 0; a < c.num_actions; ++a) {
+      const int kd = c.action_kind[a];
+      const bool raise = kd == MCCFR_ACT_RAISE_MIN || kd == MCCFR_ACT_RAISE_POT;
+      if ((k == -2 && raise) || kd == k) g.fallback[g.n_fallback++] = (uint8_t)a;
+    }
+  g.default_slot = 0;
+  for (int a = 0; a < c.num_actions; ++a)
+    if (c.action_kind[a] == MCCFR_ACT_CHECK || c.action_kind[a] == MCCFR_ACT_CHECK_CALL) {
+      g.default_slot = (uint8_t)a;
+      break;
+    }
+}
+
+int grid_for(long long work, int block) {
+  long long g = (work + block - 1) / block;
+  return (int)std::max(1LL, std::min(g, 148LL * 64));
+}
+
+int check_device_error(mccfr_handle* h) {
+  int e = 0;
+  CK(cudaMemcpy(&e, h->tv.err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    h->sticky_err |= e;
+    CK(cudaMemset(h->tv.err, 0, sizeof(int)));
+    if (e & kErrTableFull)
+      return fail(h, MCCFR_ERR_TABLE_FULL, "info-set table full (capacity %llu rows); raise table_log2", h->cap);
+    return fail(h, MCCFR_ERR_DEVICE, "kernel error flags 0x%x", e);
+  }
+  return MCCFR_OK;
+}
+
+// Enqueues one player-update (traverse + apply) reading the device schedule;
+// `ev3` (optional) receives event records before, between and after.
+int enqueue_update(mccfr_handle* h, int batch, mccfr_trace* d_trace, cudaEvent_t* ev3) {
+  const int rb = regret_frac_bits(h->cfg, batch);
+  const float rscale = std::ldexp(1.0f, rb);
+  const double rinv = std::ldexp(1.0, -rb);
+  HandView hv{h->d_hr, h->d_pre, h->d_cdf};
+  if (ev3) CK(cudaEventRecord(ev3[0], h->stream));
+  if (h->cfg.sampling == MCCFR_SAMPLING_REFERENCE) {
+    const int grid = (batch + kRefBlock - 1) / kRefBlock;
+    if (d_trace)
+      k_traverse_ref<kRefBlock, true><<<grid, kRefBlock, 0, h->stream>>>(h->gp, h->tv, hv, h->d_sched, batch,
+                                                                           rscale, h->d_counters, d_trace);
+    else
+      k_traverse_ref<kRefBlock, false><<<grid, kRefBlock, 0, h->stream>>>(h->gp, h->tv, hv, h->d_sched, batch,
+                                                                            rscale, h->d_counters, nullptr);
+  } else {
+    launch_traverse_es(h->gp, h->tv, hv, h->d_sched, batch, rscale, h->d_counters, h->stream);
+  }
+  CK(cudaGetLastError());
+  if (ev3) CK(cudaEventRecord(ev3[1], h->stream));
+  k_apply<<<148 * 8, 256, 0, h->stream>>>(h->gp, h->tv, h->d_sched, rinv);
+  CK(cudaGetLastError());
+  if (ev3) CK(cudaEventRecord(ev3[2], h->stream));
+  return MCCFR_OK;
+}
+
+int ensure_graph(mccfr_handle* h, int batch) {
+  if (h->graph && h->graph_batch == batch) return MCCFR_OK;
+  if (h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = MCCFR_OK;
+  for (int p = 0; p < h->cfg.num_players && rc == MCCFR_OK; ++p) {
+    rc = enqueue_update(h, batch, nullptr, h->gev + 3 * p);
+    if (rc == MCCFR_OK) {
+      k_advance<<<1, 1, 0, h->stream>>>(h->d_sched, h->cfg.num_players);
+      if (cudaGetLastError() != cudaSuccess) rc = MCCFR_ERR_CUDA;
+    }
+  }
+  const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+  if (rc != MCCFR_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return fail(h, MCCFR_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+  const cudaError_t e2 = cudaGraphInstantiate(&h->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e2 != cudaSuccess) return fail(h, MCCFR_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e2));
+  h->graph_batch = batch;
+  return MCCFR_OK;
+}
+
+int set_sched(mccfr_handle* h, long long iteration, int player) {
+  h->h_sched->iteration = iteration;
+  h->h_sched->player = player;
+  h->h_sched->pad = 0;
+  CK(cudaMemcpyAsync(h->d_sched, h->h_sched, sizeof(Sched), cudaMemcpyHostToDevice, h->stream));
+  return MCCFR_OK;
+}
+
+struct HostRow {
+  unsigned long long key;
+  float reg[8], ssum[8];
+  unsigned long long visits;
+};
+
+int read_rows(mccfr_handle* h, std::vector<HostRow>& rows) {
+  CK(cudaStreamSynchronize(h->stream));
+  unsigned int* d_n = nullptr;
+  CK(cudaMalloc(&d_n, sizeof(unsigned int)));
+  CK(cudaMemset(d_n, 0, sizeof(unsigned int)));
+  unsigned long long *okeys = nullptr, *ovis = nullptr;
+  float4 *oreg = nullptr, *ossum = nullptr;
+  // One pass into buffers bounded by the capacity.
+  const unsigned long long bound = h->cap;
+  cudaError_t e = cudaMalloc(&okeys, bound * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&ovis, bound * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&oreg, bound * 2 * sizeof(float4));
+  if (e == cudaSuccess) e = cudaMalloc(&ossum, bound * 2 * sizeof(float4));
+  int rc = MCCFR_OK;
+  unsigned int n = 0;
+  if (e != cudaSuccess) {
+    rc = fail(h, MCCFR_ERR_OOM, "export buffers: %s", cudaGetErrorString(e));
+  } else {
+    k_export<<<148 * 16, 256, 0, h->stream>>>(h->tv, h->cap, okeys, oreg, ossum, ovis, d_n);
+    e = cudaMemcpyAsync(&n, d_n, sizeof(n), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) rc = fail(h, MCCFR_ERR_CUDA, "export: %s", cudaGetErrorString(e));
+    if (rc == MCCFR_OK) {
+      std::vector<unsigned long long> k(n), v(n);
+      std::vector<float> r(8ull * n), s(8ull * n);
+      if (n) {
+        e = cudaMemcpy(k.data(), okeys, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(v.data(), ovis, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(r.data(), oreg, n * 32ull, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(s.data(), ossum, n * 32ull, cudaMemcpyDeviceToHost);
+      }
+      if (e != cudaSuccess) {
+        rc = fail(h, MCCFR_ERR_CUDA, "export copy: %s", cudaGetErrorString(e));
+      } else {
+        rows.resize(n);
+        for (unsigned i = 0; i < n; ++i) {
+          rows[i].key = k[i];
+          std::memcpy(rows[i].reg, &r[8ull * i], 32);
+          std::memcpy(rows[i].ssum, &s[8ull * i], 32);
+          rows[i].visits = v[i];
+        }
+        std::sort(rows.begin(), rows.end(), [](const HostRow& a, const HostRow& b) { return a.key < b.key; });
+      }
+    }
+  }
+  cudaFree(okeys);
+  cudaFree(ovis);
+  cudaFree(oreg);
+  cudaFree(ossum);
+  cudaFree(d_n);
+  return rc;
+}
+
+void release(mccfr_handle* h) {
+  if (!h) return;
+  if (h->device >= 0) cudaSetDevice(h->device);
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  if (h->persist_set) {
+    cudaCtxResetPersistingL2Cache();
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, h->persist_prev);
+  }
+  for (auto& e : h->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : h->gev)
+    if (e) cudaEventDestroy(e);
+  cudaFree(h->d_hr);
+  cudaFree(h->d_pre);
+  cudaFree(h->d_cdf);
+  cudaFree(h->d_block);
+  cudaFree(h->d_sched);
+  cudaFreeHost(h->h_sched);
+  cudaFree(h->d_counters);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* mccfr_strerror(int s) {
+  switch (s) {
+    case MCCFR_OK: return "ok";
+    case MCCFR_ERR_INVALID_ARG: return "invalid argument";
+    case MCCFR_ERR_CUDA: return "CUDA error";
+    case MCCFR_ERR_OOM: return "out of device memory";
+    case MCCFR_ERR_IO: return "file I/O error";
+    case MCCFR_ERR_FORMAT: return "bad file format";
+    case MCCFR_ERR_NO_HAND_TABLE: return "hand-rank table not loaded";
+    case MCCFR_ERR_TABLE_FULL: return "info-set table full";
+    case MCCFR_ERR_DEVICE: return "device-side error flag";
+    case MCCFR_ERR_OVERFLOW: return "accumulator range exceeded";
+    case MCCFR_ERR_CAPACITY: return "output buffer too small";
+    case MCCFR_ERR_NO_DEVICE: return "no CUDA device";
+    case MCCFR_ERR_TIMEOUT: return "timeout";
+    default: return "unknown status";
+  }
+}
+
+const char* mccfr_last_error(mccfr_handle* h) { return h ? h->last_error.c_str() : ""; }
+
+int mccfr_abi_sizes(size_t* out3) {
+  if (!out3) return MCCFR_ERR_INVALID_ARG;
+  out3[0] = sizeof(mccfr_config);
+  out3[1] = sizeof(mccfr_stats);
+  out3[2] = sizeof(mccfr_trace);
+  return MCCFR_OK;
+}
+
+int mccfr_config_init(mccfr_config* c, int preset) {
+  if (!c) return MCCFR_ERR_INVALID_ARG;
+  std::memset(c, 0, sizeof(*c));
+  c->use_cfr_plus = 1;
+  c->use_linear_cfr = 1;
+  c->device = 0;
+  if (preset == MCCFR_PRESET_REF8) {
+    // GPUCFRTrainer defaults (cfr_gpu.cuh:50-55) and the fixed 8-slot
+    // abstraction (abstraction.h:9-10, 42-53), FNV keys, depth cut 20.
+    c->num_players = 2;
+    c->starting_stack = 1000;
+    c->small_blind = 10;
+    c->big_blind = 20;
+    c->sampling = MCCFR_SAMPLING_REFERENCE;
+    c->key_mode = MCCFR_KEY_FNV26;
+    c->num_actions = 8;
+    const int kinds[8] = {MCCFR_ACT_FOLD, MCCFR_ACT_CHECK, MCCFR_ACT_CALL, MCCFR_ACT_RAISE_MIN,
+                          MCCFR_ACT_RAISE_POT, MCCFR_ACT_RAISE_POT, MCCFR_ACT_RAISE_POT, MCCFR_ACT_ALL_IN};
+    const int nums[8] = {0, 0, 0, 0, 1, 2, 1, 0}, dens[8] = {1, 1, 1, 1, 2, 3, 1, 1};
+    for (int a = 0; a < 8; ++a) {
+      c->action_kind[a] = kinds[a];
+      c->action_num[a] = nums[a];
+      c->action_den[a] = dens[a];
+    }
+    c->raise_cap = 0;
+    c->max_depth = 20;
+    c->preflop_mode = MCCFR_PREFLOP_CHEN64;
+    c->preflop_buckets = 64;
+    c->postflop_mode = MCCFR_POSTFLOP_REF_LINEAR;
+    c->postflop_buckets[0] = c->postflop_buckets[1] = c->postflop_buckets[2] = 128;
+    c->table_log2 = 24;
+    c->seed = 42;  // the reference's hard-wired seed (cfr_gpu.cuh:124)
+    return MCCFR_OK;
+  }
+  if (preset == MCCFR_PRESET_HU_20BB || preset == MCCFR_PRESET_6MAX_100BB) {
+    const bool hu = preset == MCCFR_PRESET_HU_20BB;
+    // chips: 1 BB = 100 chips
+    c->num_players = hu ? 2 : 6;
+    c->small_blind = 50;
+    c->big_blind = 100;
+    c->starting_stack = hu ? 2000 : 10000;
+    c->sampling = MCCFR_SAMPLING_EXTERNAL;
+    c->key_mode = MCCFR_KEY_ID64;
+    if (hu) {
+      const int kinds[4] = {MCCFR_ACT_FOLD, MCCFR_ACT_CHECK_CALL, MCCFR_ACT_RAISE_POT, MCCFR_ACT_ALL_IN};
+      c->num_actions = 4;
+      for (int a = 0; a < 4; ++a) {
+        c->action_kind[a] = kinds[a];
+        c->action_num[a] = 1;
+        c->action_den[a] = 1;
+      }
+      c->raise_cap = 2;
+      c->postflop_buckets[0] = c->postflop_buckets[1] = c->postflop_buckets[2] = 50;
+      c->seed = 0;
+    } else {
+      const int kinds[6] = {MCCFR_ACT_FOLD, MCCFR_ACT_CHECK_CALL, MCCFR_ACT_RAISE_POT,
+                            MCCFR_ACT_RAISE_POT, MCCFR_ACT_RAISE_POT, MCCFR_ACT_ALL_IN};
+      const int nums[6] = {0, 0, 1, 1, 2, 0}, dens[6] = {1, 1, 2, 1, 1, 1};
+      c->num_actions = 6;
+      for (int a = 0; a < 6; ++a) {
+        c->action_kind[a] = kinds[a];
+        c->action_num[a] = nums[a];
+        c->action_den[a] = dens[a];
+      }
+      c->raise_cap = 3;
+      c->postflop_buckets[0] = c->postflop_buckets[1] = c->postflop_buckets[2] = 200;
+      c->seed = 1;
+    }
+    c->max_depth = 255;
+    c->preflop_mode = MCCFR_PREFLOP_CLASS169;
+    c->preflop_buckets = 169;
+    c->postflop_mode = MCCFR_POSTFLOP_RANK_CDF;
+    // 2^26 hashed info-set keys in a 2^27-row table (load <= 1/2, never full).
+    c->key_bits = 26;
+    c->table_log2 = 27;
+    return MCCFR_OK;
+  }
+  return MCCFR_ERR_INVALID_ARG;
+}
+
+int mccfr_create(const mccfr_config* cfg, mccfr_handle** out) {
+  if (!cfg || !out) return MCCFR_ERR_INVALID_ARG;
+  *out = nullptr;
+  std::string why;
+  if (validate(*cfg, why)) {
+    fprintf(stderr, "mccfr_create: %s\n", why.c_str());
+    return MCCFR_ERR_INVALID_ARG;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MCCFR_ERR_NO_DEVICE;
+  if (cfg->device < 0 || cfg->device >= ndev) return MCCFR_ERR_INVALID_ARG;
+  mccfr_handle* h = new mccfr_handle();
+  h->cfg = *cfg;
+  h->device = cfg->device;
+  make_params(*cfg, h->gp);
+  auto bail = [&](int rc) {
+    fprintf(stderr, "mccfr_create: %s\n", h->last_error.c_str());
+    release(h);
+    return rc;
+  };
+#define CKC(call)                                                                         \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return bail(fail(h, e_ == cudaErrorMemoryAllocation ? MCCFR_ERR_OOM : MCCFR_ERR_CUDA, \
+                       "%s: %s", #call, cudaGetErrorString(e_)));                         \
+  } while (0)
+  CKC(cudaSetDevice(h->device));
+  CKC(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  for (auto& e : h->ev) CKC(cudaEventCreate(&e));
+  for (auto& e : h->gev) CKC(cudaEventCreate(&e));
+  uint8_t pre[52 * 52];
+  build_preflop_lut(cfg->preflop_mode, cfg->preflop_buckets, pre);
+  CKC(cudaMalloc(&h->d_pre, sizeof(pre)));
+  CKC(cudaMemcpy(h->d_pre, pre, sizeof(pre), cudaMemcpyHostToDevice));
+  CKC(cudaMalloc(&h->d_cdf, 3 * 7463));
+  CKC(cudaMemset(h->d_cdf, 0, 3 * 7463));
+  CKC(cudaMalloc(&h->d_sched, sizeof(Sched)));
+  CKC(cudaMallocHost(&h->h_sched, sizeof(Sched)));
+  CKC(cudaMalloc(&h->d_counters, sizeof(Counters)));
+  CKC(cudaMemset(h->d_counters, 0, sizeof(Counters)));
+  // Table arrays in one allocation.
+  h->cap = 1ull << cfg->table_log2;
+  const unsigned long long C = h->cap;
+  const size_t bytes_keys = C * 8, bytes_reg = C * 32, bytes_ssum = C * 32, bytes_vis = C * 8,
+               bytes_tag = C * 8, bytes_cnt = C * 8, bytes_su = C * 8, bytes_da = C * 64, bytes_ds = C * 64,
+               bytes_touch = C * 4, bytes_misc = 256;
+  const size_t total = bytes_keys + bytes_reg + bytes_ssum + bytes_vis + bytes_tag + bytes_cnt + bytes_su +
+                       bytes_da + bytes_ds + bytes_touch + bytes_misc;
+  CKC(cudaMalloc(&h->d_block, total));
+  CKC(cudaMemset(h->d_block, 0, total));
+  char* p = static_cast<char*>(h->d_block);
+  auto take = [&](size_t b) {
+    char* q = p;
+    p += b;
+    return q;
+  };
+  h->tv.reg = reinterpret_cast<float4*>(take(bytes_reg));
+  h->tv.ssum = reinterpret_cast<float4*>(take(bytes_ssum));
+  h->tv.da = reinterpret_cast<long long*>(take(bytes_da));
+  h->tv.ds = reinterpret_cast<long long*>(take(bytes_ds));
+  h->tv.keys = reinterpret_cast<unsigned long long*>(take(bytes_keys));
+  h->tv.visits = reinterpret_cast<unsigned long long*>(take(bytes_vis));
+  h->tv.tag = reinterpret_cast<unsigned long long*>(take(bytes_tag));
+  h->tv.cnt = reinterpret_cast<unsigned long long*>(take(bytes_cnt));
+  h->tv.su = reinterpret_cast<long long*>(take(bytes_su));
+  h->tv.touched = reinterpret_cast<unsigned int*>(take(bytes_touch));
+  char* misc = take(bytes_misc);
+  h->tv.n_touched = reinterpret_cast<unsigned int*>(misc);
+  h->tv.err = reinterpret_cast<int*>(misc + 64);
+  h->tv.mask = C - 1;
+  h->tv.log2cap = cfg->table_log2;
+  *out = h;
+  return MCCFR_OK;
+#undef CKC
+}
+
+void mccfr_destroy(mccfr_handle* h) { release(h); }
+
+int mccfr_get_config(mccfr_handle* h, mccfr_config* out) {
+  if (!h || !out) return MCCFR_ERR_INVALID_ARG;
+  *out = h->cfg;
+  return MCCFR_OK;
+}
+
+int mccfr_get_stream(mccfr_handle* h, void** stream) {
+  if (!h || !stream) return MCCFR_ERR_INVALID_ARG;
+  *stream = (void*)h->stream;
+  return MCCFR_OK;
+}
+
+int mccfr_set_hand_table(mccfr_handle* h, const int32_t* table, size_t n) {
+  if (!h || !table) return MCCFR_ERR_INVALID_ARG;
+  if (n != (size_t)MCCFR_HAND_TABLE_ENTRIES)
+    return fail(h, MCCFR_ERR_FORMAT, "expected %d int32 entries, found %zu", MCCFR_HAND_TABLE_ENTRIES, n);
+  // Known answer of the reference's loader (cfr_gpu.cu:270-299).
+  {
+    const int seq[7] = {51, 50, 49, 48, 47, 0, 14};
+    auto rm = [](int c) { return (c % 13) * 4 + c / 13 + 1; };
+    long long p = 53;
+    bool ok = true;
+    for (int i = 0; i < 7 && ok; ++i) {
+      const long long idx = p + rm(seq[i]);
+      if (idx < 0 || idx >= (long long)n) ok = false;
+      else p = table[idx];
+    }
+    if (!ok || decode_packed((int32_t)(p & 0xFFFF)) != 7462)
+      return fail(h, MCCFR_ERR_FORMAT, "As Ks Qs Js Ts 2c 3d does not decode to 7462");
+  }
+  CK(cudaSetDevice(h->device));
+  const size_t bytes = n * sizeof(int32_t);
+  if (!h->d_hr) CK(cudaMalloc(&h->d_hr, bytes));
+  CK(cudaMemcpy(h->d_hr, table, bytes, cudaMemcpyHostToDevice));
+  // Rank-CDF bucket LUTs from exact histograms.
+  if (h->cfg.postflop_mode == MCCFR_POSTFLOP_RANK_CDF) {
+    unsigned long long* d_hist = nullptr;
+    CK(cudaMalloc(&d_hist, 7463 * sizeof(unsigned long long)));
+    uint8_t lut[3][7463];
+    for (int s = 0; s < 3; ++s) {
+      CK(cudaMemset(d_hist, 0, 7463 * sizeof(unsigned long long)));
+      k_rank_hist<<<(52 * 52 * 52 + 127) / 128, 128, 0, h->stream>>>(h->d_hr, 5 + s, d_hist);
+      CK(cudaGetLastError());
+      unsigned long long hist[7463];
+      CK(cudaMemcpyAsync(hist, d_hist, sizeof(hist), cudaMemcpyDeviceToHost, h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+      build_cdf_lut(hist, h->cfg.postflop_buckets[s], lut[s]);
+    }
+    cudaFree(d_hist);
+    CK(cudaMemcpy(h->d_cdf, lut, sizeof(lut), cudaMemcpyHostToDevice));
+  }
+  // Keep the rank table in L2 with a persisting access-policy window, as far as
+  // the device's set-aside allows.  Restored in mccfr_destroy.
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, h->device));
+  const char* env = getenv("MCCFR_L2_PERSIST");
+  const bool want = !(env && env[0] == '0');
+  if (want && prop.persistingL2CacheMaxSize > 0 && prop.accessPolicyMaxWindowSize > 0) {
+    if (!h->persist_set) {
+      size_t prev = 0;
+      cudaDeviceGetLimit(&prev, cudaLimitPersistingL2CacheSize);
+      h->persist_prev = prev;
+      h->persist_set = true;
+    }
+    const size_t setaside = std::min<size_t>(prop.persistingL2CacheMaxSize, bytes);
+    CK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, setaside));
+    cudaStreamAttrValue attr;
+    std::memset(&attr, 0, sizeof(attr));
+    const size_t win = std::min<size_t>(prop.accessPolicyMaxWindowSize, bytes);
+    attr.accessPolicyWindow.base_ptr = h->d_hr;
+    attr.accessPolicyWindow.num_bytes = win;
+    attr.accessPolicyWindow.hitRatio = std::min(1.0f, (float)setaside / (float)win);
+    attr.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    attr.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    CK(cudaStreamSetAttribute(h->stream, cudaStreamAttributeAccessPolicyWindow, &attr));
+    if (h->graph) {  // policies are baked into captured kernel nodes
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+      h->graph_batch = -1;
+    }
+  }
+  h->has_table = true;
+  return MCCFR_OK;
+}
+
+int mccfr_load_hand_table(mccfr_handle* h, const char* path) {
+  if (!h || !path) return MCCFR_ERR_INVALID_ARG;
+  FILE* f = fopen(path, "rb");
+  if (!f) return fail(h, MCCFR_ERR_IO, "cannot open %s", path);
+  fseek(f, 0, SEEK_END);
+  const long sz = ftell(f);
+  fseek(f, 0, SEEK_SET);
+  if (sz != (long)MCCFR_HAND_TABLE_ENTRIES * 4) {
+    fclose(f);
+    return fail(h, MCCFR_ERR_FORMAT, "%s: expected %d int32 entries, found %ld bytes", path,
+                MCCFR_HAND_TABLE_ENTRIES, sz);
+  }
+  std::vector<int32_t> t(MCCFR_HAND_TABLE_ENTRIES);
+  const size_t r = fread(t.data(), 4, t.size(), f);
+  fclose(f);
+  if (r != t.size()) return fail(h, MCCFR_ERR_IO, "%s: short read", path);
+  return mccfr_set_hand_table(h, t.data(), t.size());
+}
+
+int mccfr_step(mccfr_handle* h, long long iteration, int player, int batch, mccfr_trace* trace) {
+  if (!h || iteration < 1 || player < 0 || player >= h->cfg.num_players || batch < 1)
+    return MCCFR_ERR_INVALID_ARG;
+  if (!h->has_table) return fail(h, MCCFR_ERR_NO_HAND_TABLE, "load a hand-rank table first");
+  if (trace && h->cfg.sampling != MCCFR_SAMPLING_REFERENCE)
+    return fail(h, MCCFR_ERR_INVALID_ARG, "traces are recorded under reference sampling only");
+  CK(cudaSetDevice(h->device));
+  mccfr_trace* d_trace = nullptr;
+  if (trace) {
+    CK(cudaMalloc(&d_trace, (size_t)batch * sizeof(mccfr_trace)));
+    CK(cudaMemsetAsync(d_trace, 0, (size_t)batch * sizeof(mccfr_trace), h->stream));
+  }
+  int rc = set_sched(h, iteration, player);
+  if (rc == MCCFR_OK) rc = enqueue_update(h, batch, d_trace, h->ev);
+  if (rc == MCCFR_OK) {
+    const cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) rc = fail(h, MCCFR_ERR_CUDA, "step: %s", cudaGetErrorString(e));
+  }
+  if (rc == MCCFR_OK) {
+    float t1 = 0, t2 = 0;
+    cudaEventElapsedTime(&t1, h->ev[0], h->ev[1]);
+    cudaEventElapsedTime(&t2, h->ev[1], h->ev[2]);
+    h->last_traverse_ms = t1;
+    h->last_apply_ms = t2;
+    h->traverse_ms += t1;
+    h->apply_ms += t2;
+    h->launches++;
+    unsigned nt[2] = {0, 0};
+    cudaMemcpy(nt, h->tv.n_touched, sizeof(nt), cudaMemcpyDeviceToHost);
+    h->touched_last = 0;  // counter already reset for the next update
+    rc = check_device_error(h);
+  }
+  if (rc == MCCFR_OK && trace) {
+    const cudaError_t e = cudaMemcpy(trace, d_trace, (size_t)batch * sizeof(mccfr_trace), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) rc = fail(h, MCCFR_ERR_CUDA, "trace copy: %s", cudaGetErrorString(e));
+  }
+  if (d_trace) cudaFree(d_trace);
+  return rc;
+}
+
+int mccfr_train(mccfr_handle* h, long long iters, int batch, int verbose, const char* ckpt_path,
+                long long ckpt_interval) {
+  if (!h || iters < 0 || batch < 1) return MCCFR_ERR_INVALID_ARG;
+  if (!h->has_table) return fail(h, MCCFR_ERR_NO_HAND_TABLE, "load a hand-rank table first");
+  if (iters == 0) return MCCFR_OK;
+  CK(cudaSetDevice(h->device));
+  int rc = ensure_graph(h, batch);
+  if (rc) return rc;
+  rc = set_sched(h, h->iterations_done + 1, 0);
+  if (rc) return rc;
+  const bool timed = (verbose & 2) != 0;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (long long i = 0; i < iters; ++i) {
+    CK(cudaGraphLaunch(h->graph, h->stream));
+    if (timed) {
+      // event nodes inside the graph bracket every traverse and apply kernel
+      const int np = h->cfg.num_players;
+      CK(cudaEventSynchronize(h->gev[3 * (np - 1) + 2]));
+      for (int p = 0; p < np; ++p) {
+        float t1 = 0, t2 = 0;
+        cudaEventElapsedTime(&t1, h->gev[3 * p], h->gev[3 * p + 1]);
+        cudaEventElapsedTime(&t2, h->gev[3 * p + 1], h->gev[3 * p + 2]);
+        h->traverse_ms += t1;
+        h->apply_ms += t2;
+        h->last_traverse_ms = t1;
+        h->last_apply_ms = t2;
+      }
+    }
+    h->launches += h->cfg.num_players;
+    const long long it = h->iterations_done + i + 1;
+    if ((verbose & 1) && (it % 100 == 0 || i + 1 == iters)) {
+      CK(cudaStreamSynchronize(h->stream));
+      const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      const double done = (double)(i + 1) * batch * h->cfg.num_players;
+      printf("\r  %lld/%lld iters  %.1fM traversals/s  ", i + 1, iters, done / sec / 1e6);
+      fflush(stdout);
+    }
+    if (ckpt_path && ckpt_path[0] && ckpt_interval > 0 && it % ckpt_interval == 0) {
+      CK(cudaStreamSynchronize(h->stream));
+      h->iterations_done = it;
+      rc = mccfr_save_checkpoint(h, ckpt_path);
+      if (rc) return rc;
+      rc = set_sched(h, it + 1, 0);
+      if (rc) return rc;
+    }
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  if (verbose & 1) printf("\n");
+  h->iterations_done += iters;
+  return check_device_error(h);
+}
+
+int mccfr_get_stats(mccfr_handle* h, mccfr_stats* out) {
+  if (!h || !out) return MCCFR_ERR_INVALID_ARG;
+  CK(cudaSetDevice(h->device));
+  std::memset(out, 0, sizeof(*out));
+  Counters c;
+  CK(cudaMemcpyAsync(&c, h->d_counters, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  out->iterations_done = h->iterations_done;
+  out->launches = h->launches;
+  out->traversals = (int64_t)c.traversals;
+  out->node_visits = (int64_t)c.visits;
+  out->traverser_updates = (int64_t)c.updates;
+  out->terminals = (int64_t)c.terminals;
+  out->hand_evals = (int64_t)c.evals;
+  out->table_capacity = (int64_t)h->cap;
+  out->traverse_ms = h->traverse_ms;
+  out->apply_ms = h->apply_ms;
+  out->last_traverse_ms = h->last_traverse_ms;
+  out->last_apply_ms = h->last_apply_ms;
+  out->device_error = h->sticky_err;
+  out->touched_last = h->touched_last;
+  out->rows_used = -1;  // filled by mccfr_export_rows callers; counting needs a table scan
+  return MCCFR_OK;
+}
+
+int mccfr_export_rows(mccfr_handle* h, uint64_t* keys, float* regrets, float* strategy_sum, uint64_t* visits,
+                      size_t capacity, size_t* count) {
+  if (!h || !count) return MCCFR_ERR_INVALID_ARG;
+  CK(cudaSetDevice(h->device));
+  std::vector<HostRow> rows;
+  const int rc = read_rows(h, rows);
+  if (rc) return rc;
+  *count = rows.size();
+  if (capacity < rows.size()) return MCCFR_ERR_CAPACITY;
+  for (size_t i = 0; i < rows.size(); ++i) {
+    if (keys) keys[i] = rows[i].key;
+    if (regrets) std::memcpy(regrets + 8 * i, rows[i].reg, 32);
+    if (strategy_sum) std::memcpy(strategy_sum + 8 * i, rows[i].ssum, 32);
+    if (visits) visits[i] = rows[i].visits;
+  }
+  return MCCFR_OK;
+}
+
+// Average strategy (cfr_gpu.cu:1029-1058 normalisation, 1399-1411 host filter).
+int mccfr_get_strategy(mccfr_handle* h, uint32_t* keys, uint64_t* keys64, float* probs, size_t capacity,
+                       size_t* count) {
+  if (!h || !count) return MCCFR_ERR_INVALID_ARG;
+  CK(cudaSetDevice(h->device));
+  std::vector<HostRow> rows;
+  const int rc = read_rows(h, rows);
+  if (rc) return rc;
+  size_t n = 0;
+  std::vector<std::pair<unsigned long long, std::array<float, 8>>> out;
+  out.reserve(rows.size());
+  for (const HostRow& r : rows) {
+    float tot = 0.0f;
+    for (int a = 0; a < 8; ++a) tot += r.ssum[a];
+    std::array<float, 8> pr;
+    for (int a = 0; a < 8; ++a) pr[a] = (tot > 1e-7f) ? r.ssum[a] / tot : 0.0f;
+    float t2 = 0.0f;
+    for (int a = 0; a < 8; ++a) t2 += pr[a];
+    if (t2 < 1e-6f) continue;
+    out.push_back({r.key, pr});
+  }
+  n = out.size();
+  *count = n;
+  if (capacity < n) return MCCFR_ERR_CAPACITY;
+  for (size_t i = 0; i < n; ++i) {
+    const unsigned long long k = out[i].first;
+    if (keys) keys[i] = (h->cfg.key_mode == MCCFR_KEY_FNV26) ? (uint32_t)(k - 1) : (uint32_t)k;
+    if (keys64) keys64[i] = k;
+    if (probs) std::memcpy(probs + 8 * i, out[i].second.data(), 32);
+  }
+  return MCCFR_OK;
+}
+
+int mccfr_num_info_sets_active(mccfr_handle* h, long long* out) {
+  if (!h || !out) return MCCFR_ERR_INVALID_ARG;
+  std::vector<HostRow> rows;
+  const int rc = read_rows(h, rows);
+  if (rc) return rc;
+  long long n = 0;
+  for (const HostRow& r : rows)
+    for (int a = 0; a < 8; ++a)
+      if (r.ssum[a] > 0.f) {
+        ++n;
+        break;
+      }
+  *out = n;
+  return MCCFR_OK;
+}
+
+int mccfr_export_tables(mccfr_handle* h, float* regrets, float* strategy_sum, size_t n) {
+  if (!h || !regrets || !strategy_sum) return MCCFR_ERR_INVALID_ARG;
+  if (h->cfg.key_mode != MCCFR_KEY_FNV26)
+    return fail(h, MCCFR_ERR_INVALID_ARG, "dense tables exist for FNV26 keys only");
+  const size_t need = 8ull * MCCFR_REF_TABLE_SIZE;
+  if (n != need) return fail(h, MCCFR_ERR_INVALID_ARG, "expected n = %zu floats per table", need);
+  CK(cudaSetDevice(h->device));
+  float *dr = nullptr, *ds = nullptr;
+  CK(cudaMalloc(&dr, need * 4));
+  cudaError_t e = cudaMalloc(&ds, need * 4);
+  int rc = MCCFR_OK;
+  if (e != cudaSuccess) rc = fail(h, MCCFR_ERR_OOM, "dense export buffers");
+  if (!rc) {
+    cudaMemsetAsync(dr, 0, need * 4, h->stream);
+    cudaMemsetAsync(ds, 0, need * 4, h->stream);
+    k_export_dense<<<148 * 16, 256, 0, h->stream>>>(h->tv, h->cap, dr, ds, MCCFR_REF_TABLE_SIZE);
+    e = cudaMemcpyAsync(regrets, dr, need * 4, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(strategy_sum, ds, need * 4, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) rc = fail(h, MCCFR_ERR_CUDA, "dense export: %s", cudaGetErrorString(e));
+  }
+  cudaFree(dr);
+  cudaFree(ds);
+  return rc;
+}
+
+int mccfr_import_tables(mccfr_handle* h, const float* regrets, const float* strategy_sum, size_t n) {
+  if (!h || !regrets || !strategy_sum) return MCCFR_ERR_INVALID_ARG;
+  if (h->cfg.key_mode != MCCFR_KEY_FNV26)
+    return fail(h, MCCFR_ERR_INVALID_ARG, "dense tables exist for FNV26 keys only");
+  const size_t need = 8ull * MCCFR_REF_TABLE_SIZE;
+  if (n != need) return fail(h, MCCFR_ERR_INVALID_ARG, "expected n = %zu floats per table", need);
+  CK(cudaSetDevice(h->device));
+  float *dr = nullptr, *ds = nullptr;
+  CK(cudaMalloc(&dr, need * 4));
+  cudaError_t e = cudaMalloc(&ds, need * 4);
+  int rc = MCCFR_OK;
+  if (e != cudaSuccess) rc = fail(h, MCCFR_ERR_OOM, "dense import buffers");
+  if (!rc) {
+    e = cudaMemcpyAsync(dr, regrets, need * 4, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ds, strategy_sum, need * 4, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+      // Rows keep their keys; values are replaced (zeros where the dense table is zero).
+      k_import_dense<<<148 * 16, 256, 0, h->stream>>>(h->tv, dr, ds, MCCFR_REF_TABLE_SIZE);
+      e = cudaStreamSynchronize(h->stream);
+    }
+    if (e != cudaSuccess) rc = fail(h, MCCFR_ERR_CUDA, "dense import: %s", cudaGetErrorString(e));
+  }
+  cudaFree(dr);
+  cudaFree(ds);
+  if (!rc) rc = check_device_error(h);
+  return rc;
+}
+
+int mccfr_save_checkpoint(mccfr_handle* h, const char* path) {
+  if (!h || !path) return MCCFR_ERR_INVALID_ARG;
+  const size_t n = 8ull * MCCFR_REF_TABLE_SIZE;
+  std::vector<float> r(n), s(n);
+  int rc = mccfr_export_tables(h, r.data(), s.data(), n);
+  if (rc) return rc;
+  FILE* f = fopen(path, "wb");
+  if (!f) return fail(h, MCCFR_ERR_IO, "cannot open %s", path);
+  const uint64_t magic = 0x43465247505500ULL;
+  const uint32_t ts = MCCFR_REF_TABLE_SIZE, na = 8;
+  bool ok = fwrite(&magic, 8, 1, f) == 1 && fwrite(&ts, 4, 1, f) == 1 && fwrite(&na, 4, 1, f) == 1 &&
+            fwrite(r.data(), 4, n, f) == n && fwrite(s.data(), 4, n, f) == n;
+  ok = (fclose(f) == 0) && ok;
+  return ok ? MCCFR_OK : fail(h, MCCFR_ERR_IO, "write %s failed", path);
+}
+
+int mccfr_load_checkpoint(mccfr_handle* h, const char* path) {
+  if (!h || !path) return MCCFR_ERR_INVALID_ARG;
+  FILE* f = fopen(path, "rb");
+  if (!f) return fail(h, MCCFR_ERR_IO, "cannot open %s", path);
+  uint64_t magic = 0;
+  uint32_t ts = 0, na = 0;
+  bool ok = fread(&magic, 8, 1, f) == 1 && fread(&ts, 4, 1, f) == 1 && fread(&na, 4, 1, f) == 1;
+  if (!ok || magic != 0x43465247505500ULL || ts != (uint32_t)MCCFR_REF_TABLE_SIZE || na != 8) {
+    fclose(f);
+    return fail(h, MCCFR_ERR_FORMAT, "%s: not a checkpoint with table_size=2^26 and 8 actions", path);
+  }
+  const size_t n = 8ull * MCCFR_REF_TABLE_SIZE;
+  std::vector<float> r(n), s(n);
+  ok = fread(r.data(), 4, n, f) == n && fread(s.data(), 4, n, f) == n;
+  fclose(f);
+  if (!ok) return fail(h, MCCFR_ERR_FORMAT, "%s: truncated checkpoint", path);
+  const int rc = mccfr_import_tables(h, r.data(), s.data(), n);
+  if (rc) return rc;
+  if (h->cfg.use_cfr_plus) {
+    k_clamp_all<<<148 * 16, 256, 0, h->stream>>>(h->tv, h->cap);
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  return MCCFR_OK;
+}
+
+// Strategy dump v2 (strategy.cpp:6-8, 35-52), rows sorted by key.
+int mccfr_save_strategy(mccfr_handle* h, const char* path) {
+  if (!h || !path) return MCCFR_ERR_INVALID_ARG;
+  size_t n = 0;
+  int rc = mccfr_get_strategy(h, nullptr, nullptr, nullptr, 0, &n);
+  if (rc && rc != MCCFR_ERR_CAPACITY) return rc;
+  std::vector<uint32_t> k(n);
+  std::vector<float> p(8 * n);
+  rc = mccfr_get_strategy(h, k.data(), nullptr, p.data(), n, &n);
+  if (rc) return rc;
+  FILE* f = fopen(path, "wb");
+  if (!f) return fail(h, MCCFR_ERR_IO, "cannot open %s", path);
+  const uint64_t magic = 0x53545241540100ULL;
+  const uint32_t ts = MCCFR_REF_TABLE_SIZE, na = 8, cnt = (uint32_t)n;
+  bool ok = fwrite(&magic, 8, 1, f) == 1 && fwrite(&ts, 4, 1, f) == 1 && fwrite(&na, 4, 1, f) == 1 &&
+            fwrite(&cnt, 4, 1, f) == 1;
+  for (size_t i = 0; i < n && ok; ++i) ok = fwrite(&k[i], 4, 1, f) == 1 && fwrite(&p[8 * i], 4, 8, f) == 8;
+  ok = (fclose(f) == 0) && ok;
+  return ok ? MCCFR_OK : fail(h, MCCFR_ERR_IO, "write %s failed", path);
+}
+
+int mccfr_eval7_device(mccfr_handle* h, const uint8_t* dev_cards, uint16_t* dev_ranks, size_t n, float* ms) {
+  if (!h || !dev_cards || !dev_ranks) return MCCFR_ERR_INVALID_ARG;
+  if (!h->has_table) return fail(h, MCCFR_ERR_NO_HAND_TABLE, "load a hand-rank table first");
+  CK(cudaSetDevice(h->device));
+  CK(cudaEventRecord(h->ev[0], h->stream));
+  if (n) k_eval7<<<grid_for((long long)n, 256), 256, 0, h->stream>>>(h->d_hr, dev_cards, dev_ranks, n);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(h->ev[1], h->stream));
+  CK(cudaEventSynchronize(h->ev[1]));
+  if (ms) cudaEventElapsedTime(ms, h->ev[0], h->ev[1]);
+  return MCCFR_OK;
+}
+
+int mccfr_eval7(mccfr_handle* h, const uint8_t* cards, uint16_t* ranks, size_t n) {
+  if (!h || !cards || !ranks) return MCCFR_ERR_INVALID_ARG;
+  if (!h->has_table) return fail(h, MCCFR_ERR_NO_HAND_TABLE, "load a hand-rank table first");
+  if (n == 0) return MCCFR_OK;
+  for (size_t i = 0; i < 7 * n; ++i)
+    if (cards[i] > 51) return fail(h, MCCFR_ERR_INVALID_ARG, "card code %d out of range", (int)cards[i]);
+  CK(cudaSetDevice(h->device));
+  uint8_t* dc = nullptr;
+  uint16_t* dr = nullptr;
+  CK(cudaMalloc(&dc, 7 * n));
+  cudaError_t e = cudaMalloc(&dr, 2 * n);
+  int rc = MCCFR_OK;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dc, cards, 7 * n, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) rc = mccfr_eval7_device(h, dc, dr, n, nullptr);
+  if (e == cudaSuccess && !rc) e = cudaMemcpy(ranks, dr, 2 * n, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) rc = fail(h, MCCFR_ERR_CUDA, "eval7: %s", cudaGetErrorString(e));
+  cudaFree(dc);
+  cudaFree(dr);
+  return rc;
+}
+
+}  // extern "C"

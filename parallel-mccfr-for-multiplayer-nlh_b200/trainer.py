@@ -1,0 +1,168 @@
+"""Host mirror of the reference's trainer class over the C ABI.
+
+`GPUCFRTrainer` keeps the constructor, method names, argument meaning and
+return conventions of poker_cuda/src/cfr_gpu.cuh:48-132:
+  * load_hand_table / save_checkpoint / load_checkpoint return bool, as there;
+  * train(total_iterations, batch_size=65536, verbose=True, ckpt_path="",
+    ckpt_interval=10000) as cfr_gpu.cu:1244;
+  * get_strategy() returns {u32 key: float32[8]} like HostStrategyTable
+    (cfr_gpu.cuh:30-33), rows with a zero sum skipped (cfr_gpu.cu:1399-1411);
+  * num_info_sets_active(), export_tables(), import_tables().
+Where the reference calls exit(1) on a CUDA error (cfr_gpu.cu:61-69) this class
+raises MccfrError.  Extra keyword arguments select the seed, update rule and
+abstraction preset that the reference hard-wires.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import byref, c_longlong, c_size_t, c_void_p
+
+import numpy as np
+
+from . import lib as L
+
+
+class GPUCFRTrainer:
+    def __init__(self, num_players: int = 2, starting_stack: int = 1000, small_blind: int = 10,
+                 big_blind: int = 20, use_cfr_plus: bool = True, use_linear_cfr: bool = True, *,
+                 preset: int = L.PRESET_REF8, config: L.Config | None = None, seed: int | None = None,
+                 sampling: int | None = None, table_log2: int | None = None, device: int = 0):
+        self._lib = L.load()
+        if config is None:
+            config = L.preset(preset)
+            if preset == L.PRESET_REF8:
+                config.num_players = num_players
+                config.starting_stack = starting_stack
+                config.small_blind = small_blind
+                config.big_blind = big_blind
+            config.use_cfr_plus = int(bool(use_cfr_plus))
+            config.use_linear_cfr = int(bool(use_linear_cfr))
+        if seed is not None:
+            config.seed = int(seed)
+        if sampling is not None:
+            config.sampling = int(sampling)
+        if table_log2 is not None:
+            config.table_log2 = int(table_log2)
+        config.device = int(device)
+        self.config = config
+        h = c_void_p()
+        L.check(self._lib.mccfr_create(byref(config), byref(h)))
+        self._h = h
+        self.iterations_done = 0
+
+    # -- lifetime ------------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.mccfr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> c_void_p:
+        return self._h
+
+    # -- reference API -------------------------------------------------------
+    def load_hand_table(self, path: str = "data/handranks.dat") -> bool:
+        return self._lib.mccfr_load_hand_table(self._h, str(path).encode()) == L.OK
+
+    def set_hand_table(self, table: np.ndarray) -> None:
+        t = np.ascontiguousarray(table, dtype=np.int32)
+        L.check(self._lib.mccfr_set_hand_table(self._h, L.ptr(t), t.size), self._h)
+
+    def train(self, total_iterations: int, batch_size: int = 65536, verbose: bool = True,
+              ckpt_path: str = "", ckpt_interval: int = 10000, timed: bool = False) -> None:
+        flags = (1 if verbose else 0) | (2 if timed else 0)
+        L.check(self._lib.mccfr_train(self._h, int(total_iterations), int(batch_size), flags,
+                                      ckpt_path.encode(), int(ckpt_interval)), self._h)
+        self.iterations_done += int(total_iterations)
+
+    def get_strategy(self) -> dict[int, np.ndarray]:
+        keys, probs = self.strategy_arrays()
+        return {int(k): probs[i] for i, k in enumerate(keys)}
+
+    def save_checkpoint(self, path: str) -> bool:
+        return self._lib.mccfr_save_checkpoint(self._h, str(path).encode()) == L.OK
+
+    def load_checkpoint(self, path: str) -> bool:
+        return self._lib.mccfr_load_checkpoint(self._h, str(path).encode()) == L.OK
+
+    def num_info_sets_active(self) -> int:
+        n = c_longlong()
+        L.check(self._lib.mccfr_num_info_sets_active(self._h, byref(n)), self._h)
+        return int(n.value)
+
+    def export_tables(self) -> tuple[np.ndarray, np.ndarray]:
+        n = 8 * L.REF_TABLE_SIZE
+        r = np.empty(n, dtype=np.float32)
+        s = np.empty(n, dtype=np.float32)
+        L.check(self._lib.mccfr_export_tables(self._h, L.ptr(r), L.ptr(s), n), self._h)
+        return r, s
+
+    def import_tables(self, regrets: np.ndarray, strategy_sum: np.ndarray) -> None:
+        r = np.ascontiguousarray(regrets, dtype=np.float32)
+        s = np.ascontiguousarray(strategy_sum, dtype=np.float32)
+        L.check(self._lib.mccfr_import_tables(self._h, L.ptr(r), L.ptr(s), r.size), self._h)
+
+    # -- extensions ----------------------------------------------------------
+    def step(self, iteration: int, player: int, batch: int, trace: bool = False):
+        """One player-update; returns per-traversal trace records when asked."""
+        buf = np.zeros(batch, dtype=L.TRACE_DTYPE) if trace else None
+        L.check(self._lib.mccfr_step(self._h, int(iteration), int(player), int(batch),
+                                     L.ptr(buf) if trace else None), self._h)
+        return buf
+
+    def strategy_arrays(self) -> tuple[np.ndarray, np.ndarray]:
+        n = c_size_t()
+        rc = self._lib.mccfr_get_strategy(self._h, None, None, None, 0, byref(n))
+        if rc not in (L.OK, L.ERR_CAPACITY):
+            L.check(rc, self._h)
+        cap = n.value
+        keys = np.empty(cap, dtype=np.uint32)
+        probs = np.empty((cap, 8), dtype=np.float32)
+        L.check(self._lib.mccfr_get_strategy(self._h, L.ptr(keys), None, L.ptr(probs), cap, byref(n)), self._h)
+        return keys[: n.value], probs[: n.value]
+
+    def export_rows(self) -> dict[str, np.ndarray]:
+        n = c_size_t()
+        rc = self._lib.mccfr_export_rows(self._h, None, None, None, None, 0, byref(n))
+        if rc not in (L.OK, L.ERR_CAPACITY):
+            L.check(rc, self._h)
+        cap = n.value
+        keys = np.empty(cap, dtype=np.uint64)
+        reg = np.empty((cap, 8), dtype=np.float32)
+        ssum = np.empty((cap, 8), dtype=np.float32)
+        vis = np.empty(cap, dtype=np.uint64)
+        L.check(self._lib.mccfr_export_rows(self._h, L.ptr(keys), L.ptr(reg), L.ptr(ssum), L.ptr(vis), cap,
+                                            byref(n)), self._h)
+        m = n.value
+        return {"keys": keys[:m], "regrets": reg[:m], "strategy_sum": ssum[:m], "visits": vis[:m]}
+
+    def save_strategy(self, path: str) -> bool:
+        return self._lib.mccfr_save_strategy(self._h, str(path).encode()) == L.OK
+
+    def stats(self) -> L.Stats:
+        s = L.Stats()
+        L.check(self._lib.mccfr_get_stats(self._h, byref(s)), self._h)
+        return s
+
+    def stream_ptr(self) -> int:
+        p = c_void_p()
+        L.check(self._lib.mccfr_get_stream(self._h, byref(p)), self._h)
+        return int(p.value or 0)
+
+    def eval7(self, cards: np.ndarray) -> np.ndarray:
+        c = np.ascontiguousarray(cards, dtype=np.uint8).reshape(-1, 7)
+        out = np.empty(c.shape[0], dtype=np.uint16)
+        L.check(self._lib.mccfr_eval7(self._h, L.ptr(c), L.ptr(out), c.shape[0]), self._h)
+        return out

@@ -1,0 +1,89 @@
+"""The C-ABI library loads, exports every declared symbol, and its structs match
+the bindings (CPU; no compute calls)."""
+from __future__ import annotations
+
+import ctypes
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from conftest import ROOT, gpu_available, mccfr
+
+L = mccfr.lib
+HEADER = ROOT / "include" / "mccfr.h"
+
+
+def declared_functions() -> set[str]:
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return set(re.findall(r"\b(mccfr_[a-z0-9_]+)\s*\(", text))
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared_functions()
+    assert len(names) >= 25
+    out = subprocess.run(["nm", "-D", "--defined-only", str(L.LIB_PATH)], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    missing = names - exported
+    assert not missing, missing
+    lib = L.load()
+    for n in names:
+        assert getattr(lib, n) is not None
+    assert set(L.SIGNATURES) == names
+
+
+def test_struct_sizes_match():
+    sizes = (ctypes.c_size_t * 3)()
+    assert L.load().mccfr_abi_sizes(sizes) == 0
+    assert sizes[0] == ctypes.sizeof(L.Config)
+    assert sizes[1] == ctypes.sizeof(L.Stats)
+    assert sizes[2] == ctypes.sizeof(L.Trace) == L.TRACE_DTYPE.itemsize
+
+
+def test_presets():
+    ref8 = L.preset(L.PRESET_REF8)
+    assert (ref8.num_players, ref8.starting_stack, ref8.small_blind, ref8.big_blind) == (2, 1000, 10, 20)
+    assert ref8.num_actions == 8 and ref8.max_depth == 20 and ref8.seed == 42
+    assert list(ref8.action_kind) == [0, 1, 2, 4, 5, 5, 5, 6]
+    hu = L.preset(L.PRESET_HU_20BB)
+    assert hu.num_players == 2 and hu.starting_stack == 20 * hu.big_blind and hu.raise_cap == 2
+    assert hu.num_actions == 4 and list(hu.postflop_buckets) == [50, 50, 50] and hu.seed == 0
+    six = L.preset(L.PRESET_6MAX_100BB)
+    assert six.num_players == 6 and six.starting_stack == 100 * six.big_blind and six.raise_cap == 3
+    assert six.num_actions == 6 and list(six.postflop_buckets) == [200, 200, 200] and six.seed == 1
+    assert six.table_log2 == 27 and six.key_bits == 26 and six.preflop_buckets == 169
+    assert [(six.action_num[a], six.action_den[a]) for a in (2, 3, 4)] == [(1, 2), (1, 1), (2, 1)]
+    assert L.load().mccfr_config_init(ctypes.byref(L.Config()), 99) == 1
+
+
+def test_error_strings_and_invalid_args():
+    lib = L.load()
+    assert lib.mccfr_strerror(0) == b"ok"
+    assert lib.mccfr_strerror(7) == b"info-set table full"
+    h = ctypes.c_void_p()
+    bad = L.preset(L.PRESET_REF8)
+    bad.num_players = 7
+    assert lib.mccfr_create(ctypes.byref(bad), ctypes.byref(h)) == 1
+    bad = L.preset(L.PRESET_REF8)
+    bad.action_kind[0] = 2  # no fold slot left
+    assert lib.mccfr_create(ctypes.byref(bad), ctypes.byref(h)) == 1
+    assert lib.mccfr_hand_table_generate(None, 10) == 1
+    t = np.zeros(10, dtype=np.int32)
+    assert lib.mccfr_hand_table_generate(L.ptr(t), 10) == 2
+
+
+def test_create_without_gpu_fails_cleanly():
+    if gpu_available():
+        return
+    h = ctypes.c_void_p()
+    cfg = L.preset(L.PRESET_REF8)
+    assert L.load().mccfr_create(ctypes.byref(cfg), ctypes.byref(h)) == L.ERR_NO_DEVICE
+    try:
+        mccfr.GPUCFRTrainer()
+    except mccfr.MccfrError as e:
+        assert e.status == L.ERR_NO_DEVICE
+    else:
+        raise AssertionError("expected MccfrError")

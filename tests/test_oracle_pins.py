@@ -1,0 +1,90 @@
+"""The oracle's restatements against the reference's own functions and against
+published known answers (CPU)."""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+import binding
+from conftest import mccfr
+
+L = mccfr.lib
+PINS = Path(__file__).parent / "golden" / "ref_pins.npz"
+
+
+def test_philox_known_answers():
+    """Philox4x32-10 known-answer vectors of the Random123 distribution
+    (Salmon et al., SC'11)."""
+    kat = [
+        ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+        ((0xFFFFFFFF,) * 4, (0xFFFFFFFF,) * 2, (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+        ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+         (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)),
+    ]
+    for ctr, key, want in kat:
+        assert tuple(int(x) for x in binding.philox(ctr, key)) == want
+
+
+def test_uniform_mapping():
+    u = binding.lib().orc_uniform01
+    assert u(0) == 2.0 ** -24
+    assert u(0xFFFFFFFF) == 1.0
+    assert u(0x80000000) == (2 ** 23 + 1) * 2.0 ** -24
+
+
+def test_preflop_buckets_match_reference():
+    pins = np.load(PINS)
+    lut = binding.preflop_lut(L.PREFLOP_CHEN64, 64).reshape(52, 52)
+    assert np.array_equal(lut, pins["pre"])
+    c169 = binding.preflop_lut(L.PREFLOP_CLASS169, 169).reshape(52, 52)
+    ids = {int(c169[a, b]) for a in range(52) for b in range(52) if a != b}
+    assert ids == set(range(169))
+
+
+def test_action_rules_match_reference():
+    pins = np.load(PINS)
+    cfg = L.preset(L.PRESET_REF8)
+    for s, m, ch in zip(pins["states"], pins["masks"], pins["chips"]):
+        pot, stack, to_call, cb, lfr, bb = map(int, s)
+        cfg.big_blind = bb
+        assert binding.valid_mask(cfg, pot, stack, to_call, cb, lfr) == int(m)
+        for a in range(8):
+            assert binding.chips(cfg, a, pot, stack, to_call, cb, lfr) == int(ch[a])
+
+
+def test_postflop_buckets_follow_gpu_rule(hand_table):
+    """The reference's GPU bucket (cfr_gpu.cu:487-488) truncates to 8 bits while
+    its CPU twin (abstraction.cpp:71-72) clamps at 127: they agree whenever the
+    unclamped value is below 127, and the oracle follows the GPU."""
+    pins = np.load(PINS)
+    cards = pins["cards"]
+    lib = binding.lib()
+    agree = 0
+    for i in range(cards.shape[0]):
+        h0, h1 = int(cards[i, 0]), int(cards[i, 1])
+        comm = np.ascontiguousarray(cards[i, 2:])
+        for st in (1, 2, 3):
+            o = lib.orc_ref_board_bucket(L.ptr(hand_table), h0, h1, L.ptr(comm), st, 128)
+            cpu = int(pins["fast"][i, st - 1])
+            if cpu < 127:
+                assert o == cpu
+                agree += 1
+    assert agree > 0.4 * 3 * cards.shape[0]
+
+
+def test_rank_cdf_buckets_are_monotone(hand_table):
+    for n, b in ((5, 50), (6, 200), (7, 200)):
+        out = np.zeros(7463, dtype=np.uint8)
+        binding.lib().orc_rank_cdf_lut(L.ptr(hand_table), n, b, L.ptr(out))
+        assert np.all(np.diff(out[1:].astype(int)) >= 0)
+        assert out[1] == 0 and out[7462] == b - 1
+
+
+def test_regret_fraction_bits():
+    cfg = L.preset(L.PRESET_6MAX_100BB)
+    rb = binding.lib().orc_regret_frac_bits(ctypes.byref(cfg), 1 << 20)
+    # batch * 64 visits * 20 * N * stack * 2^rb must stay below 2^61
+    assert 8 <= rb <= 24
+    assert (1 << 20) * 64 * 20 * 6 * 10000 * (1 << rb) < (1 << 63)
