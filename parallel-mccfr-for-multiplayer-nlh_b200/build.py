@@ -57,6 +57,22 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     return LIB
 
 
+CLI = PKG / "mccfr_cli"
+
+
+def build_cli(force: bool = False) -> Path:
+    """The command-line front end (reference flag names), linked to libmccfr.so."""
+    deps = [CSRC / "cli.cpp", ROOT / "include" / "mccfr_trainer.hpp", ROOT / "include" / "mccfr.h", LIB]
+    if not force and not _stale(CLI, deps):
+        return CLI
+    cuda_home = Path(_nvcc()).resolve().parent.parent
+    cmd = ["g++", "-O2", "-std=c++17", str(CSRC / "cli.cpp"), f"-I{cuda_home / 'include'}", f"-L{PKG}", "-lmccfr",
+           f"-L{cuda_home / 'lib64'}", "-lcudart", "-Wl,-rpath,$ORIGIN", f"-Wl,-rpath,{cuda_home / 'lib64'}",
+           "-o", str(CLI)]
+    subprocess.run(cmd, check=True)
+    return CLI
+
+
 def build_oracle(force: bool = False) -> Path:
     """Builds oracle/liboracle.so and, when the reference sources are present,
     oracle/_ref/libref.so (test infrastructure only)."""
@@ -72,6 +88,7 @@ def build_oracle(force: bool = False) -> Path:
 
 def build_all(force: bool = False, verbose: bool = False) -> None:
     build_library(force=force, verbose=verbose)
+    build_cli(force=force)
     build_oracle(force=force)
 
 

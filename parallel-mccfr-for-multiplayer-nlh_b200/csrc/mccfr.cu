@@ -327,7 +327,9 @@ int validate(const mccfr_config& c, std::string& why) {
   if (c.key_bits < 0 || c.key_bits > 48) return why = "key_bits must be 0..48", 1;
   // Reference rule walks one path; its records hold the updating player's nodes.
   if (c.sampling == MCCFR_SAMPLING_REFERENCE && c.raise_cap == 0 && c.max_depth > 2 * kMaxRec)
-    return why = "reference sampling without a raise cap needs max_depth <= 64", 1;
+    return why = "reference sampling without a raise cap needs max_depth <= 48", 1;
+  if (c.sampling == MCCFR_SAMPLING_REFERENCE && c.raise_cap > 0 && 4 * (c.raise_cap + 1) > kMaxRec)
+    return why = "reference sampling needs raise_cap <= 5", 1;
   return 0;
 }
 
@@ -397,14 +399,21 @@ int check_device_error(mccfr_handle* h) {
   return MCCFR_OK;
 }
 
+// Records `e` on the handle's stream; inside a stream capture this must be an
+// external record so that it becomes an event node of the graph.
+int record(mccfr_handle* h, cudaEvent_t e, bool capturing) {
+  CK(capturing ? cudaEventRecordWithFlags(e, h->stream, cudaEventRecordExternal) : cudaEventRecord(e, h->stream));
+  return MCCFR_OK;
+}
+
 // Enqueues one player-update (traverse + apply) reading the device schedule;
 // `ev3` (optional) receives event records before, between and after.
-int enqueue_update(mccfr_handle* h, int batch, mccfr_trace* d_trace, cudaEvent_t* ev3) {
+int enqueue_update(mccfr_handle* h, int batch, mccfr_trace* d_trace, cudaEvent_t* ev3, bool capturing = false) {
   const int rb = regret_frac_bits(h->cfg, batch);
   const float rscale = std::ldexp(1.0f, rb);
   const double rinv = std::ldexp(1.0, -rb);
   HandView hv{h->d_hr, h->d_pre, h->d_cdf};
-  if (ev3) CK(cudaEventRecord(ev3[0], h->stream));
+  if (ev3 && record(h, ev3[0], capturing)) return MCCFR_ERR_CUDA;
   if (h->cfg.sampling == MCCFR_SAMPLING_REFERENCE) {
     const int grid = (batch + kRefBlock - 1) / kRefBlock;
     if (d_trace)
@@ -417,10 +426,10 @@ int enqueue_update(mccfr_handle* h, int batch, mccfr_trace* d_trace, cudaEvent_t
     launch_traverse_es(h->gp, h->tv, hv, h->d_sched, batch, rscale, h->d_counters, h->stream);
   }
   CK(cudaGetLastError());
-  if (ev3) CK(cudaEventRecord(ev3[1], h->stream));
+  if (ev3 && record(h, ev3[1], capturing)) return MCCFR_ERR_CUDA;
   k_apply<<<148 * 8, 256, 0, h->stream>>>(h->gp, h->tv, h->d_sched, rinv);
   CK(cudaGetLastError());
-  if (ev3) CK(cudaEventRecord(ev3[2], h->stream));
+  if (ev3 && record(h, ev3[2], capturing)) return MCCFR_ERR_CUDA;
   return MCCFR_OK;
 }
 
@@ -434,7 +443,7 @@ int ensure_graph(mccfr_handle* h, int batch) {
   CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   int rc = MCCFR_OK;
   for (int p = 0; p < h->cfg.num_players && rc == MCCFR_OK; ++p) {
-    rc = enqueue_update(h, batch, nullptr, h->gev + 3 * p);
+    rc = enqueue_update(h, batch, nullptr, h->gev + 3 * p, true);
     if (rc == MCCFR_OK) {
       k_advance<<<1, 1, 0, h->stream>>>(h->d_sched, h->cfg.num_players);
       if (cudaGetLastError() != cudaSuccess) rc = MCCFR_ERR_CUDA;
@@ -871,7 +880,8 @@ int mccfr_step(mccfr_handle* h, long long iteration, int player, int batch, mccf
     h->launches++;
     unsigned nt[2] = {0, 0};
     cudaMemcpy(nt, h->tv.n_touched, sizeof(nt), cudaMemcpyDeviceToHost);
-    h->touched_last = 0;  // counter already reset for the next update
+    // the apply kernel resets the other parity's counter, not this one
+    h->touched_last = nt[(uint32_t)((iteration - 1) * h->cfg.num_players + player) & 1];
     rc = check_device_error(h);
   }
   if (rc == MCCFR_OK && trace) {

@@ -77,46 +77,6 @@ __device__ __forceinline__ void es_apply(const GameParams& G, EsState& s, int pl
   }
 }
 
-__device__ __forceinline__ float es_showdown(const GameParams& G, const EsState& s, int up, const uint32_t* rank) {
-  const int N = G.N;
-  int levels[kMaxPlayers];
-  int nL = 0;
-  for (int p = 0; p < N; ++p) {
-    const int v = s.inv[p];
-    if (v == 0) continue;
-    bool dup = false;
-    for (int j = 0; j < nL; ++j) dup |= (levels[j] == v);
-    if (!dup) levels[nL++] = v;
-  }
-  for (int i = 0; i < nL; ++i)
-    for (int j = i + 1; j < nL; ++j)
-      if (levels[j] < levels[i]) {
-        const int t = levels[i];
-        levels[i] = levels[j];
-        levels[j] = t;
-      }
-  float payoff = -(float)s.inv[up];
-  int prev = 0;
-  for (int li = 0; li < nL; ++li) {
-    const int L = levels[li];
-    int layer = 0;
-    uint32_t best = 0;
-    for (int q = 0; q < N; ++q) {
-      layer += max(0, min((int)s.inv[q], L) - prev);
-      if (!((s.folded >> q) & 1) && s.inv[q] >= L) best = max(best, rank[q]);
-    }
-    if (best > 0) {
-      int nwin = 0;
-      for (int q = 0; q < N; ++q)
-        if (!((s.folded >> q) & 1) && s.inv[q] >= L && rank[q] == best) nwin++;
-      if (!((s.folded >> up) & 1) && s.inv[up] >= L && rank[up] == best)
-        payoff = __fadd_rn(payoff, __fdiv_rn((float)layer, (float)nwin));
-    }
-    prev = L;
-  }
-  return payoff;
-}
-
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 k_traverse_es(const GameParams G, const TableView tv, const HandView hv, const Sched* __restrict__ sched,
@@ -214,7 +174,8 @@ k_traverse_es(const GameParams G, const TableView tv, const HandView hv, const S
             continue;
           }
         }
-        value = es_showdown(G, cur, up, rank);
+        value = side_pot_payoff(
+            N, up, cur.folded, [&](int q) { return (int)cur.inv[q]; }, [&](int q) { return rank[q]; });
         n_term++;
         break;
       }

@@ -13,8 +13,11 @@
 //     on the set of cards, which the tests check);
 //   * the regret row of each node is read once (two float4) from a snapshot that
 //     is not modified during the launch; the updating player's nodes are recorded
-//     and, when u is known, folded into the row's fixed-point accumulators with
-//     three atomics per node (visit count, sum of u, sampled-action delta).
+//     in shared memory and, when u is known, folded into the row's fixed-point
+//     accumulators with three atomics per node (visit count, sum of u,
+//     sampled-action delta).
+// The kernel keeps no dynamically indexed per-thread arrays alive across the
+// walk (the showdown reads the per-player arrays in shared memory directly).
 #pragma once
 #include "game.cuh"
 #include "table.cuh"
@@ -38,7 +41,7 @@ struct Counters {
   unsigned long long traversals, visits, updates, terminals, evals;
 };
 
-constexpr int kMaxRec = 32;
+constexpr int kMaxRec = 24;
 
 __device__ __forceinline__ void warp_add_counters(Counters* c, unsigned t, unsigned v, unsigned u,
                                                   unsigned x, unsigned e) {
@@ -151,51 +154,33 @@ __device__ __forceinline__ void deal_and_bucket(const GameParams& G, const HandV
   }
 }
 
-// Side-pot showdown for player `up` (cfr_gpu.cu:694-753).
-template <int BLOCK>
-__device__ __forceinline__ float showdown(int N, int up, uint32_t folded, const uint16_t (*s_inv)[BLOCK],
-                                          const uint16_t (*s_rank)[BLOCK], int tid) {
-  int inv[kMaxPlayers];
-  uint32_t rank[kMaxPlayers];
-#pragma unroll
-  for (int p = 0; p < kMaxPlayers; ++p) {
-    inv[p] = (p < N) ? (int)s_inv[p][tid] : 0;
-    rank[p] = (p < N && !((folded >> p) & 1)) ? (uint32_t)s_rank[p][tid] : 0u;
-  }
-  int levels[kMaxPlayers];
-  int nL = 0;
-#pragma unroll
-  for (int p = 0; p < kMaxPlayers; ++p) {
-    if (p >= N || inv[p] == 0) continue;
-    bool dup = false;
-    for (int j = 0; j < nL; ++j) dup |= (levels[j] == inv[p]);
-    if (!dup) levels[nL++] = inv[p];
-  }
-  for (int i = 0; i < nL; ++i)
-    for (int j = i + 1; j < nL; ++j)
-      if (levels[j] < levels[i]) {
-        const int tmp = levels[i];
-        levels[i] = levels[j];
-        levels[j] = tmp;
-      }
-  float payoff = -(float)inv[up];
+// Side-pot showdown for player `up` (cfr_gpu.cu:694-753).  The distinct non-zero
+// invested amounts are visited in ascending order as "the smallest amount above
+// the previous level", which is the reference's sorted level list without an
+// array; invested chips and ranks are read from the caller's per-player arrays.
+template <class InvF, class RankF>
+__device__ __forceinline__ float side_pot_payoff(int N, int up, uint32_t folded, InvF inv, RankF rank) {
+  float payoff = -(float)inv(up);
   int prev = 0;
-  for (int li = 0; li < nL; ++li) {
-    const int L = levels[li];
+  for (int guard = 0; guard < kMaxPlayers; ++guard) {
+    int L = 0x7FFFFFFF;
+    for (int q = 0; q < N; ++q) {
+      const int v = inv(q);
+      if (v > prev && v < L) L = v;
+    }
+    if (L == 0x7FFFFFFF) break;
     int layer = 0;
     uint32_t best = 0;
-#pragma unroll
-    for (int q = 0; q < kMaxPlayers; ++q) {
-      if (q >= N) continue;
-      layer += max(0, min(inv[q], L) - prev);
-      if (!((folded >> q) & 1) && inv[q] >= L) best = max(best, rank[q]);
+    for (int q = 0; q < N; ++q) {
+      const int v = inv(q);
+      layer += max(0, min(v, L) - prev);
+      if (!((folded >> q) & 1) && v >= L) best = max(best, (uint32_t)rank(q));
     }
     if (best > 0) {
       int nwin = 0;
-#pragma unroll
-      for (int q = 0; q < kMaxPlayers; ++q)
-        if (q < N && !((folded >> q) & 1) && inv[q] >= L && rank[q] == best) nwin++;
-      if (!((folded >> up) & 1) && inv[up] >= L && rank[up] == best)
+      for (int q = 0; q < N; ++q)
+        if (!((folded >> q) & 1) && inv(q) >= L && (uint32_t)rank(q) == best) nwin++;
+      if (!((folded >> up) & 1) && inv(up) >= L && (uint32_t)rank(up) == best)
         payoff = __fadd_rn(payoff, __fdiv_rn((float)layer, (float)nwin));
     }
     prev = L;
@@ -213,6 +198,10 @@ k_traverse_ref(const GameParams G, const TableView tv, const HandView hv, const 
   __shared__ uint16_t s_inv[kMaxPlayers][BLOCK];
   __shared__ uint16_t s_rank[kMaxPlayers][BLOCK];
   __shared__ uint32_t s_ctx[kMaxPlayers][BLOCK];
+  // updating-player nodes of each thread's path: slot, sampled | mask << 8, q
+  __shared__ uint32_t s_rec_slot[kMaxRec][BLOCK];
+  __shared__ uint16_t s_rec_sv[kMaxRec][BLOCK];
+  __shared__ float s_rec_q[kMaxRec][BLOCK];
 
   for (int i = threadIdx.x; i < 52 * 52 / 4; i += BLOCK)
     reinterpret_cast<uint32_t*>(s_pre)[i] = __ldg(reinterpret_cast<const uint32_t*>(hv.pre) + i);
@@ -271,9 +260,6 @@ k_traverse_ref(const GameParams G, const TableView tv, const HandView hv, const 
       if (!((allin >> p) & 1)) q |= (uint32_t)p << (4 * nq++);
     }
     // path walk
-    uint32_t rec_slot[kMaxRec];
-    uint32_t rec_sv[kMaxRec];  // sampled | vm << 8
-    float rec_q[kMaxRec];
     int nrec = 0;
     unsigned n_visits = 0, n_updates = 0;
     int n_act = 0;
@@ -313,7 +299,9 @@ k_traverse_ref(const GameParams G, const TableView tv, const HandView hv, const 
           }
         }
         if (showdown_now) {
-          u = showdown<BLOCK>(N, up, folded, s_inv, s_rank, tid);
+          u = side_pot_payoff(
+              N, up, folded, [&](int q) { return (int)s_inv[q][tid]; },
+              [&](int q) { return (uint32_t)s_rank[q][tid]; });
           break;
         }
         continue;
@@ -348,9 +336,9 @@ k_traverse_ref(const GameParams G, const TableView tv, const HandView hv, const 
         node_strategy(reg, vm, strat);
         n_updates++;
         if (nrec < kMaxRec && slot >= 0) {
-          rec_slot[nrec] = (uint32_t)slot;
-          rec_sv[nrec] = (uint32_t)s | (vm << 8);
-          rec_q[nrec] = fmaxf(strat[s], 0.05f);
+          s_rec_slot[nrec][tid] = (uint32_t)slot;
+          s_rec_sv[nrec][tid] = (uint16_t)((uint32_t)s | (vm << 8));
+          s_rec_q[nrec][tid] = fmaxf(strat[s], 0.05f);
           nrec++;
         } else if (slot >= 0) {
           atomicOr(tv.err, kErrRecordOverflow);
@@ -396,11 +384,11 @@ k_traverse_ref(const GameParams G, const TableView tv, const HandView hv, const 
     // Fold u into the recorded nodes' accumulators.
     const long long fu = fix_r(u, rscale);
     for (int i = 0; i < nrec; ++i) {
-      const uint32_t slot = rec_slot[i];
-      const uint32_t sv = rec_sv[i];
+      const uint32_t slot = s_rec_slot[i][tid];
+      const uint32_t sv = s_rec_sv[i][tid];
       const int s = (int)(sv & 0xFF);
       const uint32_t vm = sv >> 8;
-      const long long ds_ = fix_r(__fsub_rn(__fdiv_rn(u, rec_q[i]), u), rscale);
+      const long long ds_ = fix_r(__fsub_rn(__fdiv_rn(u, s_rec_q[i][tid]), u), rscale);
       if (touch_row(tv, slot, uid, vm)) {
         atomicAdd(tv.cnt + slot, (1ull << 32) | 1ull);
         atomicAdd(reinterpret_cast<unsigned long long*>(tv.su + slot), (unsigned long long)fu);

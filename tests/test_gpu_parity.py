@@ -86,7 +86,7 @@ def test_external_sampling_bit_exact(hand_table, preset, batch):
 
 
 def test_external_sampling_on_reference_game(hand_table):
-    cfg, tr, orc = make_pair(L.PRESET_REF8, hand_table, sampling=L.SAMPLING_EXTERNAL)
+    cfg, tr, orc = make_pair(L.PRESET_REF8, hand_table, table_log2=24, sampling=L.SAMPLING_EXTERNAL)
     for it in (1, 2):
         for p in range(2):
             tr.step(it, p, 1024)
