@@ -234,6 +234,21 @@ int mccfr_eval7(mccfr_handle* h, const uint8_t* cards, uint16_t* ranks, size_t n
 int mccfr_eval7_device(mccfr_handle* h, const uint8_t* dev_cards,
                        uint16_t* dev_ranks, size_t n, float* ms);
 
+/* ---- evaluation without device allocation --------------------------------
+   No counterpart in the reference.  For callers that cannot allocate device
+   memory (code inside a framework that owns every device allocation, or a
+   process that must not grow its device footprint): the same 7-card evaluation
+   as mccfr_eval7, with its staging in a static device array of
+   MCCFR_EVAL7_STATIC_MAX_HANDS hands (about 2.25 MiB, held by every GPU that
+   loads the library until exit).  dev_table is the caller's device copy of the
+   32,487,834-entry rank table; cards (7 per hand, 0..51) and ranks are host
+   buffers; runs on the current device.  n above the maximum returns
+   MCCFR_ERR_INVALID_ARG.  The first call on a device looks up the array's
+   address and must come before any stream capture.  Calls share the array, so
+   calls that overlap on the GPU race: serialise them. */
+#define MCCFR_EVAL7_STATIC_MAX_HANDS (1u << 18)
+int mccfr_eval7_static(const int32_t* dev_table, const uint8_t* cards, uint16_t* ranks, size_t n);
+
 #ifdef __cplusplus
 }
 #endif

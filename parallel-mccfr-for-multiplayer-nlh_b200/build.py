@@ -20,7 +20,7 @@ LIB = PKG / "libmccfr.so"
 ORACLE_DIR = ROOT / "oracle"
 REFERENCE_SRC = Path("/root/reference/poker_cuda/src")
 
-SOURCES = ["mccfr.cu", "handtable.cpp", "abstraction.cpp"]
+SOURCES = ["mccfr.cu", "eval_static.cu", "handtable.cpp", "abstraction.cpp"]
 HEADERS = ["game.cuh", "table.cuh", "traverse_ref.cuh", "traverse_es.cuh", "handtable.h"]
 
 NVCC_FLAGS = [

@@ -109,7 +109,9 @@ SIGNATURES = {
     "mccfr_abi_sizes": (c_int, [c_void_p]),
     "mccfr_eval7": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),
     "mccfr_eval7_device": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t, POINTER(c_float)]),
+    "mccfr_eval7_static": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),
 }
+EVAL7_STATIC_MAX_HANDS = 1 << 18
 
 _lib = None
 
