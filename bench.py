@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--batch", type=int, default=0, help="traversals per player-update (0 = workload default)")
     ap.add_argument("--no-extras", action="store_true", help="skip the secondary measurements")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--table-log2", type=int, default=0, help="override the table capacity (profiling cases)")
+    ap.add_argument("--key-bits", type=int, default=-1, help="override the hashed key width (profiling cases)")
     return ap.parse_args()
 
 
@@ -180,6 +182,10 @@ def main():
     cfg, batch = make_config(L, args.workload, rank)
     if args.batch:
         batch = args.batch
+    if args.table_log2:
+        cfg.table_log2 = args.table_log2
+    if args.key_bits >= 0:
+        cfg.key_bits = args.key_bits
     metric = "6-max traversals/s" if cfg.num_players == 6 else "traversals/s"
 
     if args.impl == "reference":

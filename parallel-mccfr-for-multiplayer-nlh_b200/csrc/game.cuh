@@ -157,21 +157,24 @@ __device__ __forceinline__ float bf16_round(float f) {
 }
 
 // BF16 current strategy (cfr_gpu.cu:318-351) and action sampling
-// (cfr_gpu.cu:510-537), both from the same regret row.
+// (cfr_gpu.cu:510-537), both from the same regret row.  The strategy of an
+// illegal slot only ever enters the sampling sums multiplied by zero, so only
+// legal slots are divided; the result is bit-identical to dividing all eight.
 __device__ __forceinline__ int sample_action(const GameParams& G, const float* reg, uint32_t vm,
                                              float u) {
-  float pos[kSlots], sum = 0.0f;
+  float sum = 0.0f;
 #pragma unroll
-  for (int a = 0; a < kSlots; ++a) {
-    pos[a] = fmaxf(0.0f, reg[a]);
-    sum = __fadd_rn(sum, pos[a]);
-  }
-  float total = 0.0f;
+  for (int a = 0; a < kSlots; ++a) sum = __fadd_rn(sum, fmaxf(0.0f, reg[a]));
+  if (!(sum > 1e-7f)) return passive_fallback(G, vm);  // every BF16 entry is 0
   float sig[kSlots];
+  float total = 0.0f;
 #pragma unroll
   for (int a = 0; a < kSlots; ++a) {
-    sig[a] = bf16_round((sum > 1e-7f) ? __fdiv_rn(pos[a], sum) : 0.0f);
-    if ((vm >> a) & 1) total = __fadd_rn(total, sig[a]);
+    sig[a] = 0.0f;
+    if ((vm >> a) & 1) {
+      sig[a] = bf16_round(__fdiv_rn(fmaxf(0.0f, reg[a]), sum));
+      total = __fadd_rn(total, sig[a]);
+    }
   }
   if (total < 1e-7f) return passive_fallback(G, vm);
   const float r = __fmul_rn(u, total);
@@ -179,26 +182,28 @@ __device__ __forceinline__ int sample_action(const GameParams& G, const float* r
   int result = -1;
 #pragma unroll
   for (int a = 0; a < kSlots; ++a) {
-    const int valid = (vm >> a) & 1;
-    cum = __fadd_rn(cum, __fmul_rn(sig[a], (float)valid));
-    if (valid && result < 0 && r <= cum) result = a;
+    if (!((vm >> a) & 1)) continue;  // adds sig * 0 = +0 in the reference
+    cum = __fadd_rn(cum, sig[a]);
+    if (result < 0 && r <= cum) result = a;
   }
   if (result < 0) result = passive_fallback(G, vm);
   return result;
 }
 
-// Regret-matched strategy of a node (cfr_gpu.cu:784-797).
+// Regret-matched strategy of a node (cfr_gpu.cu:784-797); illegal slots are 0.
 __device__ __forceinline__ void node_strategy(const float* reg, uint32_t vm, float* strat) {
-  float r[kSlots], sum_r = 0.0f;
-#pragma unroll
-  for (int a = 0; a < kSlots; ++a) {
-    r[a] = ((vm >> a) & 1) ? fmaxf(0.0f, reg[a]) : 0.0f;
-    sum_r = __fadd_rn(sum_r, r[a]);
-  }
-  const float uni = __fdiv_rn(1.0f, (float)__popc(vm));
+  float sum_r = 0.0f;
 #pragma unroll
   for (int a = 0; a < kSlots; ++a)
-    strat[a] = (sum_r > 1e-7f) ? __fdiv_rn(r[a], sum_r) : (((vm >> a) & 1) ? uni : 0.0f);
+    if ((vm >> a) & 1) sum_r = __fadd_rn(sum_r, fmaxf(0.0f, reg[a]));
+  if (sum_r > 1e-7f) {
+#pragma unroll
+    for (int a = 0; a < kSlots; ++a) strat[a] = ((vm >> a) & 1) ? __fdiv_rn(fmaxf(0.0f, reg[a]), sum_r) : 0.0f;
+  } else {
+    const float uni = __fdiv_rn(1.0f, (float)__popc(vm));
+#pragma unroll
+    for (int a = 0; a < kSlots; ++a) strat[a] = ((vm >> a) & 1) ? uni : 0.0f;
+  }
 }
 
 // Reference info-set slot (cfr_gpu.cu:165-179).

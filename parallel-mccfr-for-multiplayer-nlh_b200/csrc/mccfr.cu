@@ -55,46 +55,57 @@ __global__ void k_advance(Sched* s, int N) {
 
 // Folds one player-update's accumulators into the rows it touched and zeroes
 // them (the sparse equivalent of kernel_clamp_regrets, cfr_gpu.cu:1018-1022).
+// Eight lanes per row, lane a owning action slot a: each row field is read and
+// written as one coalesced vector, and the row's regret matching gathers the
+// eight regrets with shuffles and sums them in slot order, like node_strategy.
 __global__ void __launch_bounds__(256) k_apply(const GameParams G, const TableView tv,
                                                const Sched* __restrict__ sched, double rinv) {
-  const long long iteration = sched->iteration;
-  const uint32_t uid = (uint32_t)((iteration - 1) * G.N + sched->player);
+  const uint32_t uid = update_id(sched, G.N);
   const unsigned n = tv.n_touched[uid & 1];
-  const double w = G.lcfr ? (double)(float)iteration : 1.0;
+  const double w = G.lcfr ? (double)(float)sched->iteration : 1.0;
   const double s32 = 2.3283064365386962890625e-10;  // 2^-32
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  const int a = threadIdx.x & 7;
+  const unsigned gmask = 0xFFu << (threadIdx.x & 24);
+  const unsigned ngroups = (gridDim.x * blockDim.x) >> 3;
+  for (unsigned i = (blockIdx.x * blockDim.x + threadIdx.x) >> 3; i < n; i += ngroups) {
     const unsigned long long slot = tv.touched[i];
-    const uint32_t m = (uint32_t)(tv.tag[slot] & 0xFF);
-    const unsigned long long cnt = tv.cnt[slot];
+    const uint32_t m = (uint32_t)(*row_tag(tv, slot) & 0xFF);
+    const unsigned long long cnt = *row_cnt(tv, slot);
     const long long canon = (long long)(cnt & 0xFFFFFFFFull);
-    const long long su = tv.su[slot];
-    const float4 r0 = tv.reg[2 * slot], r1 = tv.reg[2 * slot + 1];
-    const float4 q0 = tv.ssum[2 * slot], q1 = tv.ssum[2 * slot + 1];
-    float reg[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
-    float ss[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-    float strat[8];
-    node_strategy(reg, m, strat);
-    long long* da = tv.da + 8 * slot;
-    long long* ds = tv.ds + 8 * slot;
+    const long long su = (long long)*row_su(tv, slot);
+    const unsigned flags = *row_flags(tv, slot);
+    float* regp = reinterpret_cast<float*>(row_reg(tv, slot));
+    float* ssp = reinterpret_cast<float*>(row_ssum(tv, slot));
+    long long* dap = reinterpret_cast<long long*>(row_da(tv, slot));
+    long long* dsp = reinterpret_cast<long long*>(row_ds(tv, slot));
+    const float r_a = regp[a];
+    const float s_a = ssp[a];
+    const long long da_a = dap[a];
+    const long long ds_a = (flags & 1u) ? dsp[a] : 0ll;
+    // strategy of the canonical mask from the snapshot regrets (node_strategy)
+    float sum_r = 0.0f;
 #pragma unroll
-    for (int a = 0; a < 8; ++a) {
-      const bool in = (m >> a) & 1;
-      const long long dr = da[a] - (in ? su : 0ll);
-      const long long dsv = ds[a] + (in ? canon * fix_s(strat[a]) : 0ll);
-      float r = __fadd_rn(reg[a], __double2float_rn(__dmul_rn((double)dr, rinv)));
-      if (G.cfr_plus) r = (r < 0.0f) ? 0.0f : r;
-      reg[a] = r;
-      ss[a] = __fadd_rn(ss[a], __double2float_rn(__dmul_rn(__dmul_rn((double)dsv, s32), w)));
-      da[a] = 0;
-      ds[a] = 0;
+    for (int b = 0; b < 8; ++b) {
+      const float rb = __shfl_sync(gmask, r_a, b, 8);
+      if ((m >> b) & 1) sum_r = __fadd_rn(sum_r, fmaxf(0.0f, rb));
     }
-    tv.reg[2 * slot] = make_float4(reg[0], reg[1], reg[2], reg[3]);
-    tv.reg[2 * slot + 1] = make_float4(reg[4], reg[5], reg[6], reg[7]);
-    tv.ssum[2 * slot] = make_float4(ss[0], ss[1], ss[2], ss[3]);
-    tv.ssum[2 * slot + 1] = make_float4(ss[4], ss[5], ss[6], ss[7]);
-    tv.visits[slot] += cnt >> 32;
-    tv.cnt[slot] = 0;
-    tv.su[slot] = 0;
+    const bool in = (m >> a) & 1;
+    float strat_a = 0.0f;
+    if (in) strat_a = (sum_r > 1e-7f) ? __fdiv_rn(fmaxf(0.0f, r_a), sum_r) : __fdiv_rn(1.0f, (float)__popc(m));
+    const long long dr = da_a - (in ? su : 0ll);
+    const long long dsv = ds_a + (in ? canon * fix_s(strat_a) : 0ll);
+    float r = __fadd_rn(r_a, __double2float_rn(__dmul_rn((double)dr, rinv)));
+    if (G.cfr_plus) r = (r < 0.0f) ? 0.0f : r;
+    regp[a] = r;
+    ssp[a] = __fadd_rn(s_a, __double2float_rn(__dmul_rn(__dmul_rn((double)dsv, s32), w)));
+    dap[a] = 0;
+    if (flags & 1u) dsp[a] = 0;
+    if (a == 0) {
+      *row_visits(tv, slot) += cnt >> 32;
+      *row_cnt(tv, slot) = 0;
+      *row_su(tv, slot) = 0;
+      *row_flags(tv, slot) = 0;
+    }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) tv.n_touched[(uid + 1) & 1] = 0;
 }
@@ -105,15 +116,15 @@ __global__ void k_export(const TableView tv, unsigned long long cap_slots,
                          unsigned int* __restrict__ on) {
   for (unsigned long long s = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; s < cap_slots;
        s += (unsigned long long)gridDim.x * blockDim.x) {
-    const unsigned long long k = tv.keys[s];
+    const unsigned long long k = *row_key(tv, s);
     if (!k) continue;
     const unsigned i = atomicAdd(on, 1u);
     okeys[i] = k;
-    oreg[2 * i] = tv.reg[2 * s];
-    oreg[2 * i + 1] = tv.reg[2 * s + 1];
-    ossum[2 * i] = tv.ssum[2 * s];
-    ossum[2 * i + 1] = tv.ssum[2 * s + 1];
-    ovis[i] = tv.visits[s];
+    oreg[2 * i] = row_reg(tv, s)[0];
+    oreg[2 * i + 1] = row_reg(tv, s)[1];
+    ossum[2 * i] = row_ssum(tv, s)[0];
+    ossum[2 * i + 1] = row_ssum(tv, s)[1];
+    ovis[i] = *row_visits(tv, s);
   }
 }
 
@@ -132,10 +143,10 @@ __global__ void k_import_dense(const TableView tv, const float* __restrict__ dr,
     if (!any) continue;
     const long long slot = table_insert(tv, (unsigned long long)s + 1);
     if (slot < 0) continue;
-    tv.reg[2 * slot] = make_float4(r[0], r[1], r[2], r[3]);
-    tv.reg[2 * slot + 1] = make_float4(r[4], r[5], r[6], r[7]);
-    tv.ssum[2 * slot] = make_float4(q[0], q[1], q[2], q[3]);
-    tv.ssum[2 * slot + 1] = make_float4(q[4], q[5], q[6], q[7]);
+    row_reg(tv, slot)[0] = make_float4(r[0], r[1], r[2], r[3]);
+    row_reg(tv, slot)[1] = make_float4(r[4], r[5], r[6], r[7]);
+    row_ssum(tv, slot)[0] = make_float4(q[0], q[1], q[2], q[3]);
+    row_ssum(tv, slot)[1] = make_float4(q[4], q[5], q[6], q[7]);
   }
 }
 
@@ -143,11 +154,11 @@ __global__ void k_export_dense(const TableView tv, unsigned long long cap_slots,
                                float* __restrict__ ds, unsigned n_slots) {
   for (unsigned long long s = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; s < cap_slots;
        s += (unsigned long long)gridDim.x * blockDim.x) {
-    const unsigned long long k = tv.keys[s];
+    const unsigned long long k = *row_key(tv, s);
     if (!k || k > n_slots) continue;
     const unsigned d = (unsigned)(k - 1);
-    const float* r = reinterpret_cast<const float*>(tv.reg + 2 * s);
-    const float* q = reinterpret_cast<const float*>(tv.ssum + 2 * s);
+    const float* r = reinterpret_cast<const float*>(row_reg(tv, s));
+    const float* q = reinterpret_cast<const float*>(row_ssum(tv, s));
     for (int a = 0; a < 8; ++a) {
       dr[(size_t)a * n_slots + d] = r[a];
       ds[(size_t)a * n_slots + d] = q[a];
@@ -159,11 +170,11 @@ __global__ void k_export_dense(const TableView tv, unsigned long long cap_slots,
 __global__ void k_clamp_all(const TableView tv, unsigned long long cap_slots) {
   for (unsigned long long s = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; s < cap_slots;
        s += (unsigned long long)gridDim.x * blockDim.x) {
-    float4 a = tv.reg[2 * s], b = tv.reg[2 * s + 1];
+    float4 a = row_reg(tv, s)[0], b = row_reg(tv, s)[1];
     a.x = a.x < 0.f ? 0.f : a.x; a.y = a.y < 0.f ? 0.f : a.y; a.z = a.z < 0.f ? 0.f : a.z; a.w = a.w < 0.f ? 0.f : a.w;
     b.x = b.x < 0.f ? 0.f : b.x; b.y = b.y < 0.f ? 0.f : b.y; b.z = b.z < 0.f ? 0.f : b.z; b.w = b.w < 0.f ? 0.f : b.w;
-    tv.reg[2 * s] = a;
-    tv.reg[2 * s + 1] = b;
+    row_reg(tv, s)[0] = a;
+    row_reg(tv, s)[1] = b;
   }
 }
 
@@ -239,6 +250,8 @@ struct mccfr_handle {
   TableView tv{};
   void* d_block = nullptr;  // one allocation for the table arrays
   Sched* d_sched = nullptr;
+  DealRec* d_deals = nullptr;  // one record per traversal of an update
+  int deals_cap = 0;
   Sched* h_sched = nullptr;  // pinned
   Counters* d_counters = nullptr;
   // graph of one iteration
@@ -413,17 +426,20 @@ int enqueue_update(mccfr_handle* h, int batch, mccfr_trace* d_trace, cudaEvent_t
   const float rscale = std::ldexp(1.0f, rb);
   const double rinv = std::ldexp(1.0, -rb);
   HandView hv{h->d_hr, h->d_pre, h->d_cdf};
+  if (batch > h->deals_cap) return fail(h, MCCFR_ERR_INVALID_ARG, "deal buffer smaller than the batch");
+  k_deal<<<(batch + 127) / 128, 128, 0, h->stream>>>(h->gp, hv, h->d_sched, batch, h->d_deals);
+  CK(cudaGetLastError());
   if (ev3 && record(h, ev3[0], capturing)) return MCCFR_ERR_CUDA;
   if (h->cfg.sampling == MCCFR_SAMPLING_REFERENCE) {
     const int grid = (batch + kRefBlock - 1) / kRefBlock;
     if (d_trace)
-      k_traverse_ref<kRefBlock, true><<<grid, kRefBlock, 0, h->stream>>>(h->gp, h->tv, hv, h->d_sched, batch,
-                                                                           rscale, h->d_counters, d_trace);
+      k_traverse_ref<kRefBlock, true><<<grid, kRefBlock, 0, h->stream>>>(h->gp, h->tv, h->d_deals, h->d_sched,
+                                                                           batch, rscale, h->d_counters, d_trace);
     else
-      k_traverse_ref<kRefBlock, false><<<grid, kRefBlock, 0, h->stream>>>(h->gp, h->tv, hv, h->d_sched, batch,
-                                                                            rscale, h->d_counters, nullptr);
+      k_traverse_ref<kRefBlock, false><<<grid, kRefBlock, 0, h->stream>>>(h->gp, h->tv, h->d_deals, h->d_sched,
+                                                                            batch, rscale, h->d_counters, nullptr);
   } else {
-    launch_traverse_es(h->gp, h->tv, hv, h->d_sched, batch, rscale, h->d_counters, h->stream);
+    launch_traverse_es(h->gp, h->tv, h->d_deals, h->d_sched, batch, rscale, h->d_counters, h->stream);
   }
   CK(cudaGetLastError());
   if (ev3 && record(h, ev3[1], capturing)) return MCCFR_ERR_CUDA;
@@ -433,7 +449,29 @@ int enqueue_update(mccfr_handle* h, int batch, mccfr_trace* d_trace, cudaEvent_t
   return MCCFR_OK;
 }
 
+int ensure_deals(mccfr_handle* h, int batch) {
+  if (batch <= h->deals_cap) return MCCFR_OK;
+  if (h->d_deals) {
+    CK(cudaStreamSynchronize(h->stream));
+    cudaFree(h->d_deals);
+    h->d_deals = nullptr;
+    h->deals_cap = 0;
+  }
+  CK(cudaMalloc(&h->d_deals, (size_t)batch * sizeof(DealRec)));
+  h->deals_cap = batch;
+  if (h->graph) {  // the graph captured the old buffer
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+    h->graph_batch = -1;
+  }
+  return MCCFR_OK;
+}
+
 int ensure_graph(mccfr_handle* h, int batch) {
+  {
+    const int rc = ensure_deals(h, batch);
+    if (rc) return rc;
+  }
   if (h->graph && h->graph_batch == batch) return MCCFR_OK;
   if (h->graph) {
     cudaGraphExecDestroy(h->graph);
@@ -545,6 +583,7 @@ void release(mccfr_handle* h) {
   cudaFree(h->d_pre);
   cudaFree(h->d_cdf);
   cudaFree(h->d_block);
+  cudaFree(h->d_deals);
   cudaFree(h->d_sched);
   cudaFreeHost(h->h_sched);
   cudaFree(h->d_counters);
@@ -709,33 +748,16 @@ int mccfr_create(const mccfr_config* cfg, mccfr_handle** out) {
   CKC(cudaMallocHost(&h->h_sched, sizeof(Sched)));
   CKC(cudaMalloc(&h->d_counters, sizeof(Counters)));
   CKC(cudaMemset(h->d_counters, 0, sizeof(Counters)));
-  // Table arrays in one allocation.
+  // Table rows, the touched list and small counters in one allocation.
   h->cap = 1ull << cfg->table_log2;
   const unsigned long long C = h->cap;
-  const size_t bytes_keys = C * 8, bytes_reg = C * 32, bytes_ssum = C * 32, bytes_vis = C * 8,
-               bytes_tag = C * 8, bytes_cnt = C * 8, bytes_su = C * 8, bytes_da = C * 64, bytes_ds = C * 64,
-               bytes_touch = C * 4, bytes_misc = 256;
-  const size_t total = bytes_keys + bytes_reg + bytes_ssum + bytes_vis + bytes_tag + bytes_cnt + bytes_su +
-                       bytes_da + bytes_ds + bytes_touch + bytes_misc;
-  CKC(cudaMalloc(&h->d_block, total));
-  CKC(cudaMemset(h->d_block, 0, total));
-  char* p = static_cast<char*>(h->d_block);
-  auto take = [&](size_t b) {
-    char* q = p;
-    p += b;
-    return q;
-  };
-  h->tv.reg = reinterpret_cast<float4*>(take(bytes_reg));
-  h->tv.ssum = reinterpret_cast<float4*>(take(bytes_ssum));
-  h->tv.da = reinterpret_cast<long long*>(take(bytes_da));
-  h->tv.ds = reinterpret_cast<long long*>(take(bytes_ds));
-  h->tv.keys = reinterpret_cast<unsigned long long*>(take(bytes_keys));
-  h->tv.visits = reinterpret_cast<unsigned long long*>(take(bytes_vis));
-  h->tv.tag = reinterpret_cast<unsigned long long*>(take(bytes_tag));
-  h->tv.cnt = reinterpret_cast<unsigned long long*>(take(bytes_cnt));
-  h->tv.su = reinterpret_cast<long long*>(take(bytes_su));
-  h->tv.touched = reinterpret_cast<unsigned int*>(take(bytes_touch));
-  char* misc = take(bytes_misc);
+  const size_t bytes_rows = C * kRowBytes, bytes_touch = C * 4, bytes_misc = 256;
+  CKC(cudaMalloc(&h->d_block, bytes_rows + bytes_touch + bytes_misc));
+  CKC(cudaMemset(h->d_block, 0, bytes_rows + bytes_touch + bytes_misc));
+  char* base = static_cast<char*>(h->d_block);
+  h->tv.rows = reinterpret_cast<unsigned char*>(base);
+  h->tv.touched = reinterpret_cast<unsigned int*>(base + bytes_rows);
+  char* misc = base + bytes_rows + bytes_touch;
   h->tv.n_touched = reinterpret_cast<unsigned int*>(misc);
   h->tv.err = reinterpret_cast<int*>(misc + 64);
   h->tv.mask = C - 1;
@@ -863,7 +885,8 @@ int mccfr_step(mccfr_handle* h, long long iteration, int player, int batch, mccf
     CK(cudaMalloc(&d_trace, (size_t)batch * sizeof(mccfr_trace)));
     CK(cudaMemsetAsync(d_trace, 0, (size_t)batch * sizeof(mccfr_trace), h->stream));
   }
-  int rc = set_sched(h, iteration, player);
+  int rc = ensure_deals(h, batch);
+  if (rc == MCCFR_OK) rc = set_sched(h, iteration, player);
   if (rc == MCCFR_OK) rc = enqueue_update(h, batch, d_trace, h->ev);
   if (rc == MCCFR_OK) {
     const cudaError_t e = cudaStreamSynchronize(h->stream);

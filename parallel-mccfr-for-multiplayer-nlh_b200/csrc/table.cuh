@@ -1,33 +1,31 @@
 // table.cuh — open-addressed info-set table in HBM.
 //
 // Replaces the reference's direct-mapped SoA tables [8 x 2^26] (cfr_gpu.cu:
-// 1106-1136).  Rows are addressed by linear probing over 64-bit keys (0 = empty)
-// in aligned groups of four keys (one 32-byte sector per probe step).  Each row
-// has:
-//   reg[8]  float  regrets (two float4: one 32-byte sector)
-//   ssum[8] float  average-strategy sums
-//   visits  u64    updates received since creation
-// and per-player-update accumulators, zeroed by the apply kernel:
-//   tag     u64    ((update id + 1) << 8) | canonical action mask of that update
-//   cnt     u64    (all visits << 32) | visits whose mask equals the canonical one
-//   su      i64    sum of fix(u) over canonical visits (reference rule)
-//   da[8]   i64    per-action regret deltas (fixed point, 2^-rb units)
-//   ds[8]   i64    per-action strategy-sum deltas of non-canonical visits (2^-32)
+// 1106-1136).  Each row is one 256-byte record (two 128-byte lines), so that a
+// visit touches two adjacent sectors and folding a row in reads one contiguous
+// record instead of a dozen scattered ones:
+//     0  key    u64   0 = empty; linear probing from the key's home slot
+//     8  tag    u64   ((update id + 1) << 8) | canonical action mask of that update
+//    16  cnt    u64   (all visits << 32) | visits whose mask is the canonical one
+//    24  su     i64   sum of fix(u) (reference rule) or fix(v_h) (external sampling)
+//    32  reg[8] f32   regrets: read by every visit (snapshot within an update)
+//    64  ssum[8] f32  average-strategy sums
+//    96  da[8]  i64   per-action regret deltas, 2^-rb units
+//   160  ds[8]  i64   strategy weights of non-canonical visits, 2^-32 units
+//   224  visits u64   updates received since creation
+//   232  flags  u32   bit 0: ds holds values
+// tag/cnt/su/da/ds/flags are per-update accumulators, zeroed by the apply kernel.
 #pragma once
 #include <cstdint>
 
 namespace mccfr {
 
+constexpr int kRowBytes = 256;
+constexpr int kOffKey = 0, kOffTag = 8, kOffCnt = 16, kOffSu = 24, kOffReg = 32, kOffSsum = 64, kOffDa = 96,
+              kOffDs = 160, kOffVisits = 224, kOffFlags = 232;
+
 struct TableView {
-  unsigned long long* keys;
-  float4* reg;    // [cap][2]
-  float4* ssum;   // [cap][2]
-  unsigned long long* visits;
-  unsigned long long* tag;
-  unsigned long long* cnt;
-  long long* su;
-  long long* da;  // [cap][8]
-  long long* ds;  // [cap][8]
+  unsigned char* rows;       // [cap][256]
   unsigned int* touched;     // [cap]
   unsigned int* n_touched;   // [2], indexed by update-id parity
   unsigned long long mask;   // cap - 1
@@ -43,43 +41,67 @@ enum : int {
 
 constexpr int kProbeLimit = 1 << 14;
 
+__device__ __forceinline__ unsigned char* row_ptr(const TableView& tv, unsigned long long s) {
+  return tv.rows + (s << 8);
+}
+__device__ __forceinline__ unsigned long long* row_key(const TableView& tv, unsigned long long s) {
+  return reinterpret_cast<unsigned long long*>(row_ptr(tv, s) + kOffKey);
+}
+__device__ __forceinline__ unsigned long long* row_tag(const TableView& tv, unsigned long long s) {
+  return reinterpret_cast<unsigned long long*>(row_ptr(tv, s) + kOffTag);
+}
+__device__ __forceinline__ unsigned long long* row_cnt(const TableView& tv, unsigned long long s) {
+  return reinterpret_cast<unsigned long long*>(row_ptr(tv, s) + kOffCnt);
+}
+__device__ __forceinline__ unsigned long long* row_su(const TableView& tv, unsigned long long s) {
+  return reinterpret_cast<unsigned long long*>(row_ptr(tv, s) + kOffSu);
+}
+__device__ __forceinline__ float4* row_reg(const TableView& tv, unsigned long long s) {
+  return reinterpret_cast<float4*>(row_ptr(tv, s) + kOffReg);
+}
+__device__ __forceinline__ float4* row_ssum(const TableView& tv, unsigned long long s) {
+  return reinterpret_cast<float4*>(row_ptr(tv, s) + kOffSsum);
+}
+__device__ __forceinline__ unsigned long long* row_da(const TableView& tv, unsigned long long s) {
+  return reinterpret_cast<unsigned long long*>(row_ptr(tv, s) + kOffDa);
+}
+__device__ __forceinline__ unsigned long long* row_ds(const TableView& tv, unsigned long long s) {
+  return reinterpret_cast<unsigned long long*>(row_ptr(tv, s) + kOffDs);
+}
+__device__ __forceinline__ unsigned long long* row_visits(const TableView& tv, unsigned long long s) {
+  return reinterpret_cast<unsigned long long*>(row_ptr(tv, s) + kOffVisits);
+}
+__device__ __forceinline__ unsigned int* row_flags(const TableView& tv, unsigned long long s) {
+  return reinterpret_cast<unsigned int*>(row_ptr(tv, s) + kOffFlags);
+}
+
 __device__ __forceinline__ unsigned long long home_slot(const TableView& tv, unsigned long long key) {
   return (key * 0x9E3779B97F4A7C15ull) >> (64 - tv.log2cap);
 }
 
 // Read-only lookup; returns the slot or -1.
 __device__ __forceinline__ long long table_find(const TableView& tv, unsigned long long key) {
-  unsigned long long s = home_slot(tv, key) & ~3ull;
-  for (int step = 0; step < kProbeLimit; step += 4) {
-    const ulonglong2* g = reinterpret_cast<const ulonglong2*>(tv.keys + s);
-    const ulonglong2 a = __ldcg(g), b = __ldcg(g + 1);
-    if (a.x == key) return (long long)s;
-    if (a.y == key) return (long long)(s + 1);
-    if (b.x == key) return (long long)(s + 2);
-    if (b.y == key) return (long long)(s + 3);
-    if (a.x == 0 || a.y == 0 || b.x == 0 || b.y == 0) return -1;
-    s = (s + 4) & tv.mask;
+  unsigned long long s = home_slot(tv, key);
+  for (int step = 0; step < kProbeLimit; ++step) {
+    const unsigned long long k = __ldcg(row_key(tv, s));
+    if (k == key) return (long long)s;
+    if (k == 0) return -1;
+    s = (s + 1) & tv.mask;
   }
   return -1;
 }
 
 // Find or insert; returns the slot, or -1 when the probe limit is exceeded.
 __device__ __forceinline__ long long table_insert(const TableView& tv, unsigned long long key) {
-  unsigned long long s = home_slot(tv, key) & ~3ull;
-  for (int step = 0; step < kProbeLimit; step += 4) {
-    const ulonglong2* g = reinterpret_cast<const ulonglong2*>(tv.keys + s);
-    const ulonglong2 a = __ldcg(g), b = __ldcg(g + 1);
-    const unsigned long long v[4] = {a.x, a.y, b.x, b.y};
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      unsigned long long cur = v[i];
-      if (cur == key) return (long long)(s + i);
-      if (cur == 0) {
-        cur = atomicCAS(tv.keys + s + i, 0ull, key);
-        if (cur == 0 || cur == key) return (long long)(s + i);
-      }
+  unsigned long long s = home_slot(tv, key);
+  for (int step = 0; step < kProbeLimit; ++step) {
+    unsigned long long k = __ldcg(row_key(tv, s));
+    if (k == key) return (long long)s;
+    if (k == 0) {
+      k = atomicCAS(row_key(tv, s), 0ull, key);
+      if (k == 0 || k == key) return (long long)s;
     }
-    s = (s + 4) & tv.mask;
+    s = (s + 1) & tv.mask;
   }
   atomicOr(tv.err, kErrTableFull);
   return -1;
@@ -90,9 +112,10 @@ __device__ __forceinline__ long long table_insert(const TableView& tv, unsigned 
 __device__ __forceinline__ bool touch_row(const TableView& tv, unsigned long long slot, uint32_t uid,
                                           uint32_t vm) {
   const unsigned long long want = ((unsigned long long)(uid + 1) << 8) | vm;
-  unsigned long long old = __ldcg(tv.tag + slot);
+  unsigned long long* tag = row_tag(tv, slot);
+  unsigned long long old = __ldcg(tag);
   if ((old >> 8) != (unsigned long long)(uid + 1)) {
-    const unsigned long long r = atomicCAS(tv.tag + slot, old, want);
+    const unsigned long long r = atomicCAS(tag, old, want);
     if (r == old) {
       const unsigned int i = atomicAdd(tv.n_touched + (uid & 1), 1u);
       tv.touched[i] = (unsigned int)slot;
@@ -101,6 +124,18 @@ __device__ __forceinline__ bool touch_row(const TableView& tv, unsigned long lon
     old = r;
   }
   return (uint32_t)(old & 0xFF) == vm;
+}
+
+// Adds one visit whose legal mask differs from the row's canonical one: every
+// legal action's regret term and strategy weight directly.
+__device__ __forceinline__ void add_direct(const TableView& tv, unsigned long long slot, uint32_t vm,
+                                           const long long* dr, const long long* dsw) {
+  for (int a = 0; a < 8; ++a) {
+    if (!((vm >> a) & 1)) continue;
+    if (dr) atomicAdd(row_da(tv, slot) + a, (unsigned long long)dr[a]);
+    if (dsw) atomicAdd(row_ds(tv, slot) + a, (unsigned long long)dsw[a]);
+  }
+  if (dsw) atomicOr(row_flags(tv, slot), 1u);
 }
 
 }  // namespace mccfr

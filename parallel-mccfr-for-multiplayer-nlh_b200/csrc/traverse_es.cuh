@@ -79,23 +79,22 @@ __device__ __forceinline__ void es_apply(const GameParams& G, EsState& s, int pl
 
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
-k_traverse_es(const GameParams G, const TableView tv, const HandView hv, const Sched* __restrict__ sched,
+k_traverse_es(const GameParams G, const TableView tv, const DealRec* __restrict__ deals, const Sched* __restrict__ sched,
               int batch, float rscale, Counters* __restrict__ counters) {
-  __shared__ uint8_t s_pre[52 * 52];
-  for (int i = threadIdx.x; i < 52 * 52 / 4; i += BLOCK)
-    reinterpret_cast<uint32_t*>(s_pre)[i] = __ldg(reinterpret_cast<const uint32_t*>(hv.pre) + i);
-  __syncthreads();
   const uint32_t t = blockIdx.x * BLOCK + threadIdx.x;
   if (t >= (uint32_t)batch) return;
-  const long long iteration = sched->iteration;
   const int up = sched->player;
   const int N = G.N;
-  const uint32_t uid = (uint32_t)((iteration - 1) * N + up);
+  const uint32_t uid = update_id(sched, N);
 
-  uint8_t hole[2 * kMaxPlayers], board[5];
-  int dealer;
+  const DealRec& D = deals[t];
+  const int dealer = D.dealer;
   uint32_t ctx[kMaxPlayers], rank[kMaxPlayers];
-  deal_and_bucket(G, hv, s_pre, t, uid, hole, board, dealer, ctx, rank);
+#pragma unroll
+  for (int p = 0; p < kMaxPlayers; ++p) {
+    ctx[p] = D.ctx[p];
+    rank[p] = D.rank[p];
+  }
 
   EsState cur;
   {
@@ -188,14 +187,7 @@ k_traverse_es(const GameParams G, const TableView tv, const HandView hv, const S
       const unsigned long long key = info_key(G, player, hb, bkt, cur.street, cur.abits, cur.path);
       const long long slot = table_insert(tv, key);
       float reg[kSlots];
-      if (slot >= 0) {
-        const float4 r0 = __ldg(tv.reg + 2 * slot), r1 = __ldg(tv.reg + 2 * slot + 1);
-        reg[0] = r0.x; reg[1] = r0.y; reg[2] = r0.z; reg[3] = r0.w;
-        reg[4] = r1.x; reg[5] = r1.y; reg[6] = r1.z; reg[7] = r1.w;
-      } else {
-#pragma unroll
-        for (int a = 0; a < kSlots; ++a) reg[a] = 0.0f;
-      }
+      load_regrets(tv, slot, reg);
       n_visits++;
       if (player == up) {
         if (sp >= kMaxFrames || slot < 0) {
@@ -223,15 +215,15 @@ k_traverse_es(const GameParams G, const TableView tv, const HandView hv, const S
       const int s = sample_action(G, reg, vm, uniform01(d.x));
       if (slot >= 0) {
         if (touch_row(tv, (unsigned long long)slot, uid, vm)) {
-          atomicAdd(tv.cnt + slot, (1ull << 32) | 1ull);
+          atomicAdd(row_cnt(tv, slot), (1ull << 32) | 1ull);
         } else {
-          atomicAdd(tv.cnt + slot, 1ull << 32);
+          atomicAdd(row_cnt(tv, slot), 1ull << 32);
           float strat[kSlots];
           node_strategy(reg, vm, strat);
-          for (int a = 0; a < kSlots; ++a)
-            if ((vm >> a) & 1)
-              atomicAdd(reinterpret_cast<unsigned long long*>(tv.ds + 8ull * slot + a),
-                        (unsigned long long)fix_s(strat[a]));
+          long long dw[kSlots];
+#pragma unroll
+          for (int a = 0; a < kSlots; ++a) dw[a] = fix_s(strat[a]);
+          add_direct(tv, slot, vm, nullptr, dw);
         }
       }
       es_apply(G, cur, player, s);
@@ -244,8 +236,7 @@ k_traverse_es(const GameParams G, const TableView tv, const HandView hv, const S
     while (sp > 0) {
       EsFrame& F = fr[sp - 1];
       const int a = F.next_a;
-      atomicAdd(reinterpret_cast<unsigned long long*>(tv.da + 8ull * F.slot + a),
-                (unsigned long long)fix_r(value, rscale));
+      atomicAdd(row_da(tv, F.slot) + a, (unsigned long long)fix_r(value, rscale));
       F.vh = __fadd_rn(F.vh, __fmul_rn(F.strat[a], value));
       const uint32_t rest = (uint32_t)F.vm & ~((2u << a) - 1u);
       if (rest) {
@@ -260,14 +251,14 @@ k_traverse_es(const GameParams G, const TableView tv, const HandView hv, const S
       // node complete
       const float vh = F.vh;
       const long long fv = fix_r(vh, rscale);
+      atomicAdd(row_cnt(tv, F.slot), 1ull << 32);
       if (touch_row(tv, F.slot, uid, F.vm)) {
-        atomicAdd(tv.cnt + F.slot, 1ull << 32);
-        atomicAdd(reinterpret_cast<unsigned long long*>(tv.su + F.slot), (unsigned long long)fv);
+        atomicAdd(row_su(tv, F.slot), (unsigned long long)fv);
       } else {
-        atomicAdd(tv.cnt + F.slot, 1ull << 32);
-        for (int b = 0; b < kSlots; ++b)
-          if ((F.vm >> b) & 1)
-            atomicAdd(reinterpret_cast<unsigned long long*>(tv.da + 8ull * F.slot + b), (unsigned long long)(-fv));
+        long long dr[kSlots];
+#pragma unroll
+        for (int b = 0; b < kSlots; ++b) dr[b] = -fv;
+        add_direct(tv, F.slot, F.vm, dr, nullptr);
       }
       n_updates++;
       value = vh;
@@ -278,11 +269,11 @@ k_traverse_es(const GameParams G, const TableView tv, const HandView hv, const S
   warp_add_counters(counters, 1u, n_visits, n_updates, n_term, (unsigned)N);
 }
 
-inline void launch_traverse_es(const GameParams& G, const TableView& tv, const HandView& hv, const Sched* sched,
+inline void launch_traverse_es(const GameParams& G, const TableView& tv, const DealRec* deals, const Sched* sched,
                                int batch, float rscale, Counters* counters, cudaStream_t stream) {
   constexpr int B = 128;
   const int grid = (batch + B - 1) / B;
-  k_traverse_es<B><<<grid, B, 0, stream>>>(G, tv, hv, sched, batch, rscale, counters);
+  k_traverse_es<B><<<grid, B, 0, stream>>>(G, tv, deals, sched, batch, rscale, counters);
 }
 
 }  // namespace mccfr

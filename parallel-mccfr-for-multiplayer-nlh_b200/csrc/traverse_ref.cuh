@@ -1,23 +1,24 @@
-// traverse_ref.cuh — traversal kernel for the reference's update rule.
+// traverse_ref.cuh — deal kernel and the traversal kernel of the reference's rule.
 //
-// The reference runs one recursive traversal per thread with its game state in
-// local memory (cfr_gpu.cu:644-1011).  Under its rule every node samples one
-// action, so a traversal is a single root-to-terminal path and the value
-// returned by every node is the terminal payoff u (cfr_gpu.cu:809-818).  This
-// kernel therefore walks the path iteratively:
-//   * one thread per traversal; the per-player chip counts and buckets live in
-//     shared memory, column-major [field][thread] so the block's accesses are
-//     conflict-free and dynamic player indexing needs no local memory;
-//   * the deal is a counter-based Philox draw; the flop/turn/river rank chains of
-//     all players share the 3-card board prefix (the table's state depends only
-//     on the set of cards, which the tests check);
-//   * the regret row of each node is read once (two float4) from a snapshot that
-//     is not modified during the launch; the updating player's nodes are recorded
+// The reference runs one recursive traversal per thread, dealing and bucketing
+// at its start, with its game state in local memory (cfr_gpu.cu:644-1011).  Here:
+//   * k_deal deals every traversal of a player-update (counter-based Philox,
+//     the reference's partial Fisher-Yates) and computes its buckets and river
+//     ranks into a 64-byte record; the rank chains of all players share the
+//     3-card board prefix (the table's state depends only on the set of cards,
+//     which the tests check);
+//   * under the reference's rule every node samples one action, so a traversal
+//     is a single root-to-terminal path and every node on it returns the
+//     terminal payoff u (cfr_gpu.cu:809-818): k_traverse_ref walks the path
+//     iteratively, one thread per traversal, with per-player chip counts and
+//     buckets in shared memory (column-major [field][thread], conflict-free,
+//     indexable by player without local memory);
+//   * each node reads its regret row once (a 32-byte sector) from a snapshot
+//     that the update does not modify; the updating player's nodes are recorded
 //     in shared memory and, when u is known, folded into the row's fixed-point
-//     accumulators with three atomics per node (visit count, sum of u,
-//     sampled-action delta).
-// The kernel keeps no dynamically indexed per-thread arrays alive across the
-// walk (the showdown reads the per-player arrays in shared memory directly).
+//     accumulators with three atomics (visit count, sum of u, sampled-action
+//     delta).
+// No dynamically indexed per-thread array stays alive across the walk.
 #pragma once
 #include "game.cuh"
 #include "table.cuh"
@@ -36,6 +37,17 @@ struct HandView {
   const uint8_t* pre;     // preflop LUT [52*52]
   const uint8_t* cdf;     // rank-CDF LUTs [3][7463]
 };
+
+// One traversal's deal.  ctx[p] = hole bucket | flop << 8 | turn << 16 | river << 24.
+struct DealRec {
+  uint32_t ctx[kMaxPlayers];
+  uint16_t rank[kMaxPlayers];
+  uint8_t hole[2 * kMaxPlayers];
+  uint8_t board[5];
+  uint8_t dealer;
+  uint8_t pad[10];
+};
+static_assert(sizeof(DealRec) == 64, "deal record is one 64-byte pair of sectors");
 
 struct Counters {
   unsigned long long traversals, visits, updates, terminals, evals;
@@ -60,14 +72,22 @@ __device__ __forceinline__ void warp_add_counters(Counters* c, unsigned t, unsig
   }
 }
 
-// Deals the hand for traversal t of update `uid` and computes buckets and river
-// ranks.  Writes hole/board to the out arrays.
-__device__ __forceinline__ void deal_and_bucket(const GameParams& G, const HandView& hv,
-                                                const uint8_t* s_pre, uint32_t t, uint32_t uid,
-                                                uint8_t* hole, uint8_t* board, int& dealer,
-                                                uint32_t* ctx_out /*[N] packed buckets*/,
-                                                uint32_t* rank_out /*[N]*/) {
+__device__ __forceinline__ uint32_t update_id(const Sched* s, int N) {
+  return (uint32_t)((s->iteration - 1) * N + s->player);
+}
+
+// Deal, buckets and river ranks of traversal t of update `uid`
+// (cfr_gpu.cu:460-470, 476-489, 942-952, 963).
+__global__ void __launch_bounds__(128) k_deal(const GameParams G, const HandView hv, const Sched* __restrict__ sched,
+                                              int batch, DealRec* __restrict__ out) {
+  __shared__ uint8_t s_pre[52 * 52];
+  for (int i = threadIdx.x; i < 52 * 52 / 4; i += blockDim.x)
+    reinterpret_cast<uint32_t*>(s_pre)[i] = __ldg(reinterpret_cast<const uint32_t*>(hv.pre) + i);
+  __syncthreads();
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (uint32_t)batch) return;
   const int N = G.N;
+  const uint32_t uid = update_id(sched, N);
   const int n_deal = 2 * N + 5;
   uint32_t words[24];
   const int nblk = (n_deal + 1 + 3) / 4;
@@ -81,8 +101,6 @@ __device__ __forceinline__ void deal_and_bucket(const GameParams& G, const HandV
       words[4 * j + 3] = o.w;
     }
   }
-  // Partial Fisher-Yates with multiply-shift (cfr_gpu.cu:460-470), on a deck
-  // held as 52 bytes in registers/local memory.
   uint8_t deck[52];
 #pragma unroll
   for (int i = 0; i < 52; ++i) deck[i] = (uint8_t)i;
@@ -92,72 +110,64 @@ __device__ __forceinline__ void deal_and_bucket(const GameParams& G, const HandV
     deck[i] = deck[j];
     deck[j] = tmp;
   }
-  for (int i = 0; i < 2 * N; ++i) hole[i] = deck[i];
+  DealRec r;
 #pragma unroll
-  for (int i = 0; i < 5; ++i) board[i] = deck[2 * N + i];
-  dealer = (int)(words[n_deal] % (uint32_t)N);
+  for (int i = 0; i < 2 * kMaxPlayers; ++i) r.hole[i] = (i < 2 * N) ? deck[i] : 0;
+#pragma unroll
+  for (int i = 0; i < 5; ++i) r.board[i] = deck[2 * N + i];
+  r.dealer = (uint8_t)(words[n_deal] % (uint32_t)N);
+#pragma unroll
+  for (int i = 0; i < 10; ++i) r.pad[i] = 0;
 
-  // Rank chains: board prefix once, then two hole cards and the turn/river per
-  // player, all players' gathers issued together.
   const int32_t* T = hv.hr;
-  int32_t b = __ldg(T + 53 + to_rm(board[0]));
-  b = __ldg(T + b + to_rm(board[1]));
-  b = __ldg(T + b + to_rm(board[2]));
-  int32_t s5[kMaxPlayers], s6[kMaxPlayers], r7[kMaxPlayers];
-  int32_t s4[kMaxPlayers];
+  int32_t b = __ldg(T + 53 + to_rm(r.board[0]));
+  b = __ldg(T + b + to_rm(r.board[1]));
+  b = __ldg(T + b + to_rm(r.board[2]));
+  int32_t s5[kMaxPlayers], s6[kMaxPlayers], r7[kMaxPlayers], s4[kMaxPlayers];
 #pragma unroll
   for (int p = 0; p < kMaxPlayers; ++p)
-    if (p < N) s4[p] = __ldg(T + b + to_rm(hole[2 * p]));
+    if (p < N) s4[p] = __ldg(T + b + to_rm(r.hole[2 * p]));
 #pragma unroll
   for (int p = 0; p < kMaxPlayers; ++p)
-    if (p < N) s5[p] = __ldg(T + s4[p] + to_rm(hole[2 * p + 1]));
-  const int rm3 = to_rm(board[3]), rm4 = to_rm(board[4]);
+    if (p < N) s5[p] = __ldg(T + s4[p] + to_rm(r.hole[2 * p + 1]));
+  const int rm3 = to_rm(r.board[3]), rm4 = to_rm(r.board[4]);
 #pragma unroll
   for (int p = 0; p < kMaxPlayers; ++p)
     if (p < N) s6[p] = __ldg(T + s5[p] + rm3);
 #pragma unroll
   for (int p = 0; p < kMaxPlayers; ++p)
     if (p < N) r7[p] = __ldg(T + s6[p] + rm4);
-  if (G.postflop_mode == 0) {
 #pragma unroll
-    for (int p = 0; p < kMaxPlayers; ++p) {
-      if (p < N) {
-        const uint32_t hb = s_pre[hole[2 * p] * 52 + hole[2 * p + 1]];
-        const uint32_t rr = decode16((uint32_t)r7[p] & 0xFFFF);
-        const uint32_t b1 = ref_linear_bucket(decode16((uint32_t)s5[p] & 0xFFFF), G.post_b[0]);
-        const uint32_t b2 = ref_linear_bucket(decode16((uint32_t)s6[p] & 0xFFFF), G.post_b[1]);
-        const uint32_t b3 = ref_linear_bucket(rr, G.post_b[2]);
-        ctx_out[p] = hb | (b1 << 8) | (b2 << 16) | (b3 << 24);
-        rank_out[p] = rr;
-      }
+  for (int p = 0; p < kMaxPlayers; ++p) {
+    r.ctx[p] = 0;
+    r.rank[p] = 0;
+    if (p >= N) continue;
+    const uint32_t hb = s_pre[r.hole[2 * p] * 52 + r.hole[2 * p + 1]];
+    const uint32_t rr = decode16((uint32_t)r7[p] & 0xFFFF);
+    uint32_t b1, b2, b3;
+    if (G.postflop_mode == 0) {
+      // the reference decodes the 5th/6th chain value (a state) as a rank
+      b1 = ref_linear_bucket(decode16((uint32_t)s5[p] & 0xFFFF), G.post_b[0]);
+      b2 = ref_linear_bucket(decode16((uint32_t)s6[p] & 0xFFFF), G.post_b[1]);
+      b3 = ref_linear_bucket(rr, G.post_b[2]);
+    } else {
+      b1 = __ldg(hv.cdf + decode16((uint32_t)__ldg(T + s5[p]) & 0xFFFF));
+      b2 = __ldg(hv.cdf + 7463 + decode16((uint32_t)__ldg(T + s6[p]) & 0xFFFF));
+      b3 = __ldg(hv.cdf + 2 * 7463 + rr);
     }
-  } else {
-    int32_t v5[kMaxPlayers], v6[kMaxPlayers];
-#pragma unroll
-    for (int p = 0; p < kMaxPlayers; ++p)
-      if (p < N) {
-        v5[p] = __ldg(T + s5[p]);
-        v6[p] = __ldg(T + s6[p]);
-      }
-#pragma unroll
-    for (int p = 0; p < kMaxPlayers; ++p) {
-      if (p < N) {
-        const uint32_t hb = s_pre[hole[2 * p] * 52 + hole[2 * p + 1]];
-        const uint32_t rr = decode16((uint32_t)r7[p] & 0xFFFF);
-        const uint32_t b1 = __ldg(hv.cdf + decode16((uint32_t)v5[p] & 0xFFFF));
-        const uint32_t b2 = __ldg(hv.cdf + 7463 + decode16((uint32_t)v6[p] & 0xFFFF));
-        const uint32_t b3 = __ldg(hv.cdf + 2 * 7463 + rr);
-        ctx_out[p] = hb | (b1 << 8) | (b2 << 16) | (b3 << 24);
-        rank_out[p] = rr;
-      }
-    }
+    r.ctx[p] = hb | (b1 << 8) | (b2 << 16) | (b3 << 24);
+    r.rank[p] = (uint16_t)rr;
   }
+  const uint4* src = reinterpret_cast<const uint4*>(&r);
+  uint4* dst = reinterpret_cast<uint4*>(out + t);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) dst[i] = src[i];
 }
 
 // Side-pot showdown for player `up` (cfr_gpu.cu:694-753).  The distinct non-zero
 // invested amounts are visited in ascending order as "the smallest amount above
 // the previous level", which is the reference's sorted level list without an
-// array; invested chips and ranks are read from the caller's per-player arrays.
+// array; invested chips and ranks are read through the caller's accessors.
 template <class InvF, class RankF>
 __device__ __forceinline__ float side_pot_payoff(int N, int up, uint32_t folded, InvF inv, RankF rank) {
   float payoff = -(float)inv(up);
@@ -188,11 +198,22 @@ __device__ __forceinline__ float side_pot_payoff(int N, int up, uint32_t folded,
   return payoff;
 }
 
+__device__ __forceinline__ void load_regrets(const TableView& tv, long long slot, float* reg) {
+  if (slot >= 0) {
+    const float4* p = row_reg(tv, (unsigned long long)slot);
+    const float4 r0 = __ldg(p), r1 = __ldg(p + 1);
+    reg[0] = r0.x; reg[1] = r0.y; reg[2] = r0.z; reg[3] = r0.w;
+    reg[4] = r1.x; reg[5] = r1.y; reg[6] = r1.z; reg[7] = r1.w;
+  } else {
+#pragma unroll
+    for (int a = 0; a < kSlots; ++a) reg[a] = 0.0f;
+  }
+}
+
 template <int BLOCK, bool TRACE>
 __global__ void __launch_bounds__(BLOCK)
-k_traverse_ref(const GameParams G, const TableView tv, const HandView hv, const Sched* __restrict__ sched,
+k_traverse_ref(const GameParams G, const TableView tv, const DealRec* __restrict__ deals, const Sched* __restrict__ sched,
                int batch, float rscale, Counters* __restrict__ counters, mccfr_trace* __restrict__ trace) {
-  __shared__ uint8_t s_pre[52 * 52];
   __shared__ uint16_t s_stack[kMaxPlayers][BLOCK];
   __shared__ uint16_t s_bet[kMaxPlayers][BLOCK];
   __shared__ uint16_t s_inv[kMaxPlayers][BLOCK];
@@ -203,234 +224,208 @@ k_traverse_ref(const GameParams G, const TableView tv, const HandView hv, const 
   __shared__ uint16_t s_rec_sv[kMaxRec][BLOCK];
   __shared__ float s_rec_q[kMaxRec][BLOCK];
 
-  for (int i = threadIdx.x; i < 52 * 52 / 4; i += BLOCK)
-    reinterpret_cast<uint32_t*>(s_pre)[i] = __ldg(reinterpret_cast<const uint32_t*>(hv.pre) + i);
-  __syncthreads();
-
   const int tid = threadIdx.x;
   const uint32_t t = blockIdx.x * BLOCK + tid;
   if (t >= (uint32_t)batch) return;
-
-  const long long iteration = sched->iteration;
-  const int up = sched->player;
   const int N = G.N;
-  const uint32_t uid = (uint32_t)((iteration - 1) * N + up);
+  const int up = sched->player;
+  const uint32_t uid = update_id(sched, N);
 
-  uint8_t hole[2 * kMaxPlayers], board[5];
-  int dealer;
-  uint32_t ctx[kMaxPlayers], rank[kMaxPlayers];
-  deal_and_bucket(G, hv, s_pre, t, uid, hole, board, dealer, ctx, rank);
+  const DealRec& D = deals[t];
+  const int dealer = D.dealer;
 #pragma unroll
   for (int p = 0; p < kMaxPlayers; ++p)
     if (p < N) {
-      s_ctx[p][tid] = ctx[p];
-      s_rank[p][tid] = (uint16_t)rank[p];
+      s_ctx[p][tid] = D.ctx[p];
+      s_rank[p][tid] = D.rank[p];
+      s_stack[p][tid] = (uint16_t)G.stack;
+      s_bet[p][tid] = 0;
+      s_inv[p][tid] = 0;
     }
 
   // Blinds and preflop queue (cfr_gpu.cu:954-981).
   int pot, cb, lfr = G.bb, raises = 0, street = 0;
   uint32_t folded = 0, allin = 0, abits = 0;
   uint64_t path = kPathSeed;
-#pragma unroll
-  for (int p = 0; p < kMaxPlayers; ++p)
-    if (p < N) {
-      s_stack[p][tid] = (uint16_t)G.stack;
-      s_bet[p][tid] = 0;
-      s_inv[p][tid] = 0;
-    }
-  {
-    const int sbp = (N == 2) ? dealer : (dealer + 1) % N;
-    const int bbp = (N == 2) ? (dealer + 1) % N : (dealer + 2) % N;
-    const int sba = min(G.sb, G.stack), bba = min(G.bb, G.stack);
-    s_stack[sbp][tid] = (uint16_t)(G.stack - sba);
-    s_bet[sbp][tid] = (uint16_t)sba;
-    s_inv[sbp][tid] = (uint16_t)sba;
-    s_stack[bbp][tid] = (uint16_t)(G.stack - bba);
-    s_bet[bbp][tid] = (uint16_t)bba;
-    s_inv[bbp][tid] = (uint16_t)bba;
-    pot = sba + bba;
-    cb = bba;
-    if (G.stack - sba == 0) allin |= 1u << sbp;
-    if (G.stack - bba == 0) allin |= 1u << bbp;
-    // queue: 4-bit entries
-    uint32_t q = 0;
-    int nq = 0;
-    for (int i = 0; i < N; ++i) {
-      const int p = (bbp + 1 + i) % N;
-      if (!((allin >> p) & 1)) q |= (uint32_t)p << (4 * nq++);
-    }
-    // path walk
-    int nrec = 0;
-    unsigned n_visits = 0, n_updates = 0;
-    int n_act = 0;
-    float u = 0.0f;
-    int depth = 0;
-    const uint32_t all_players = (1u << N) - 1;
-    for (;;) {
-      if (depth >= G.max_depth) {
-        u = 0.0f;
-        break;
-      }
-      const uint32_t live = all_players & ~folded;
-      if (__popc(live) == 1) {
-        const int winner = __ffs(live) - 1;
-        u = (winner == up) ? (float)(pot - (int)s_inv[up][tid]) : (float)(-(int)s_inv[up][tid]);
-        break;
-      }
-      if (nq == 0) {
-        bool showdown_now = true;
-        if (street < 3) {
-          street++;
-#pragma unroll
-          for (int p = 0; p < kMaxPlayers; ++p)
-            if (p < N) s_bet[p][tid] = 0;
-          cb = 0;
-          lfr = G.bb;
-          raises = 0;
-          q = 0;
-          nq = 0;
-          for (int i = 1; i <= N; ++i) {
-            const int p = (dealer + i) % N;
-            if (!((folded >> p) & 1) && !((allin >> p) & 1)) q |= (uint32_t)p << (4 * nq++);
-          }
-          if (nq > 0) {
-            depth++;
-            showdown_now = false;
-          }
-        }
-        if (showdown_now) {
-          u = side_pot_payoff(
-              N, up, folded, [&](int q) { return (int)s_inv[q][tid]; },
-              [&](int q) { return (uint32_t)s_rank[q][tid]; });
-          break;
-        }
-        continue;
-      }
-      // Decision node.
-      const int player = (int)(q & 0xF);
-      const int pstack = s_stack[player][tid];
-      const int pbet = s_bet[player][tid];
-      const int to_call = cb - pbet;
-      const uint32_t vm = valid_mask(G, pot, pstack, to_call, cb, lfr, raises);
-      const uint32_t cw = s_ctx[player][tid];
-      const uint32_t hb = cw & 0xFF;
-      const uint32_t bkt = street ? ((cw >> (8 * street)) & 0xFF) : 0u;
-      const unsigned long long key = info_key(G, player, hb, bkt, street, abits, path);
-      const bool is_up = (player == up);
-      long long slot = is_up ? table_insert(tv, key) : table_find(tv, key);
-      float reg[kSlots];
-      if (slot >= 0) {
-        const float4 r0 = __ldg(tv.reg + 2 * slot), r1 = __ldg(tv.reg + 2 * slot + 1);
-        reg[0] = r0.x; reg[1] = r0.y; reg[2] = r0.z; reg[3] = r0.w;
-        reg[4] = r1.x; reg[5] = r1.y; reg[6] = r1.z; reg[7] = r1.w;
-      } else {
-#pragma unroll
-        for (int a = 0; a < kSlots; ++a) reg[a] = 0.0f;
-      }
-      n_visits++;
-      const U4 d = philox(U4{t, uid, (uint32_t)path, (uint32_t)(path >> 32) | 0x80000000u}, G.seed_lo,
-                          G.seed_hi);
-      const int s = sample_action(G, reg, vm, uniform01(d.x));
-      if (is_up) {
-        float strat[kSlots];
-        node_strategy(reg, vm, strat);
-        n_updates++;
-        if (nrec < kMaxRec && slot >= 0) {
-          s_rec_slot[nrec][tid] = (uint32_t)slot;
-          s_rec_sv[nrec][tid] = (uint16_t)((uint32_t)s | (vm << 8));
-          s_rec_q[nrec][tid] = fmaxf(strat[s], 0.05f);
-          nrec++;
-        } else if (slot >= 0) {
-          atomicOr(tv.err, kErrRecordOverflow);
-        }
-      }
-      if (TRACE) {
-        if (n_act < 40) trace[t].actions[n_act] = (uint8_t)s;
-      }
-      n_act++;
-      // pop the actor, apply (cfr_gpu.cu:803-807, 543-585)
-      q >>= 4;
-      nq--;
-      const int chips = chips_for(G, s, pot, pstack, to_call, cb, lfr);
-      abits = ((abits << 3) | (uint32_t)s) & 0x3FFFFFFFu;
-      path = path_step(path, s);
-      const int k = G.kind[s];
-      if (k == 0) {
-        folded |= 1u << player;
-      } else if (k != 1) {
-        const int nstack = pstack - chips, nbet = pbet + chips;
-        s_stack[player][tid] = (uint16_t)nstack;
-        s_bet[player][tid] = (uint16_t)nbet;
-        s_inv[player][tid] = (uint16_t)(s_inv[player][tid] + chips);
-        pot += chips;
-        if (nstack == 0) allin |= 1u << player;
-        if (nbet > cb) {
-          const int prev = cb;
-          const int rs = nbet - prev;
-          if (rs >= lfr || prev == 0) lfr = rs;
-          cb = nbet;
-          raises++;
-          q = 0;
-          nq = 0;
-          for (int i = 1; i < N; ++i) {
-            const int p = (player + i) % N;
-            if (!((folded >> p) & 1) && !((allin >> p) & 1)) q |= (uint32_t)p << (4 * nq++);
-          }
-        }
-      }
-      depth++;
-    }
+  const int sbp = (N == 2) ? dealer : (dealer + 1) % N;
+  const int bbp = (N == 2) ? (dealer + 1) % N : (dealer + 2) % N;
+  const int sba = min(G.sb, G.stack), bba = min(G.bb, G.stack);
+  s_stack[sbp][tid] = (uint16_t)(G.stack - sba);
+  s_bet[sbp][tid] = (uint16_t)sba;
+  s_inv[sbp][tid] = (uint16_t)sba;
+  s_stack[bbp][tid] = (uint16_t)(G.stack - bba);
+  s_bet[bbp][tid] = (uint16_t)bba;
+  s_inv[bbp][tid] = (uint16_t)bba;
+  pot = sba + bba;
+  cb = bba;
+  if (G.stack - sba == 0) allin |= 1u << sbp;
+  if (G.stack - bba == 0) allin |= 1u << bbp;
+  uint32_t q = 0;  // action queue, 4-bit entries
+  int nq = 0;
+  for (int i = 0; i < N; ++i) {
+    const int p = (bbp + 1 + i) % N;
+    if (!((allin >> p) & 1)) q |= (uint32_t)p << (4 * nq++);
+  }
 
-    // Fold u into the recorded nodes' accumulators.
-    const long long fu = fix_r(u, rscale);
-    for (int i = 0; i < nrec; ++i) {
-      const uint32_t slot = s_rec_slot[i][tid];
-      const uint32_t sv = s_rec_sv[i][tid];
-      const int s = (int)(sv & 0xFF);
-      const uint32_t vm = sv >> 8;
-      const long long ds_ = fix_r(__fsub_rn(__fdiv_rn(u, s_rec_q[i][tid]), u), rscale);
-      if (touch_row(tv, slot, uid, vm)) {
-        atomicAdd(tv.cnt + slot, (1ull << 32) | 1ull);
-        atomicAdd(reinterpret_cast<unsigned long long*>(tv.su + slot), (unsigned long long)fu);
-        atomicAdd(reinterpret_cast<unsigned long long*>(tv.da + 8ull * slot + s),
-                  (unsigned long long)(ds_ + fu));
-      } else {
-        // Mask differs from the row's canonical one (an FNV slot shared by
-        // states with different legal actions): add every term directly.
-        atomicAdd(tv.cnt + slot, 1ull << 32);
-        const float4 r0 = __ldg(tv.reg + 2 * slot), r1 = __ldg(tv.reg + 2 * slot + 1);
-        const float reg[kSlots] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
+  int nrec = 0;
+  unsigned n_visits = 0, n_updates = 0;
+  int n_act = 0;
+  float u = 0.0f;
+  int depth = 0;
+  const uint32_t all_players = (1u << N) - 1;
+  for (;;) {
+    if (depth >= G.max_depth) {
+      u = 0.0f;
+      break;
+    }
+    const uint32_t live = all_players & ~folded;
+    if (__popc(live) == 1) {
+      const int winner = __ffs(live) - 1;
+      u = (winner == up) ? (float)(pot - (int)s_inv[up][tid]) : (float)(-(int)s_inv[up][tid]);
+      break;
+    }
+    if (nq == 0) {
+      bool showdown_now = true;
+      if (street < 3) {
+        street++;
+#pragma unroll
+        for (int p = 0; p < kMaxPlayers; ++p)
+          if (p < N) s_bet[p][tid] = 0;
+        cb = 0;
+        lfr = G.bb;
+        raises = 0;
+        q = 0;
+        nq = 0;
+        for (int i = 1; i <= N; ++i) {
+          const int p = (dealer + i) % N;
+          if (!((folded >> p) & 1) && !((allin >> p) & 1)) q |= (uint32_t)p << (4 * nq++);
+        }
+        if (nq > 0) {
+          depth++;
+          showdown_now = false;
+        }
+      }
+      if (showdown_now) {
+        u = side_pot_payoff(
+            N, up, folded, [&](int x) { return (int)s_inv[x][tid]; }, [&](int x) { return (uint32_t)s_rank[x][tid]; });
+        break;
+      }
+      continue;
+    }
+    // Decision node.
+    const int player = (int)(q & 0xF);
+    const int pstack = s_stack[player][tid];
+    const int pbet = s_bet[player][tid];
+    const int to_call = cb - pbet;
+    const uint32_t vm = valid_mask(G, pot, pstack, to_call, cb, lfr, raises);
+    const uint32_t cw = s_ctx[player][tid];
+    const uint32_t hb = cw & 0xFF;
+    const uint32_t bkt = street ? ((cw >> (8 * street)) & 0xFF) : 0u;
+    const unsigned long long key = info_key(G, player, hb, bkt, street, abits, path);
+    const bool is_up = (player == up);
+    const long long slot = is_up ? table_insert(tv, key) : table_find(tv, key);
+    float reg[kSlots];
+    load_regrets(tv, slot, reg);
+    n_visits++;
+    const U4 d = philox(U4{t, uid, (uint32_t)path, (uint32_t)(path >> 32) | 0x80000000u}, G.seed_lo, G.seed_hi);
+    const int s = sample_action(G, reg, vm, uniform01(d.x));
+    if (is_up) {
+      n_updates++;
+      if (nrec < kMaxRec && slot >= 0) {
         float strat[kSlots];
         node_strategy(reg, vm, strat);
-        for (int a = 0; a < kSlots; ++a) {
-          if (!((vm >> a) & 1)) continue;
-          atomicAdd(reinterpret_cast<unsigned long long*>(tv.da + 8ull * slot + a),
-                    (unsigned long long)(a == s ? ds_ : -fu));
-          atomicAdd(reinterpret_cast<unsigned long long*>(tv.ds + 8ull * slot + a),
-                    (unsigned long long)fix_s(strat[a]));
-        }
+        s_rec_slot[nrec][tid] = (uint32_t)slot;
+        s_rec_sv[nrec][tid] = (uint16_t)((uint32_t)s | (vm << 8));
+        s_rec_q[nrec][tid] = fmaxf(strat[s], 0.05f);
+        nrec++;
+      } else if (slot >= 0) {
+        atomicOr(tv.err, kErrRecordOverflow);
       }
     }
     if (TRACE) {
-      mccfr_trace& tr = trace[t];
-      for (int i = 0; i < 12; ++i) tr.hole[i] = (i < 2 * N) ? hole[i] : 0;
-      for (int i = 0; i < 5; ++i) tr.board[i] = board[i];
-      tr.dealer = (uint8_t)dealer;
-      tr.n_actions = (uint8_t)n_act;
-      tr.n_traverser_nodes = (uint8_t)nrec;
-      for (int p = 0; p < 6; ++p) {
-        const uint32_t cw = (p < N) ? ctx[p] : 0u;
-        tr.hole_bucket[p] = (uint8_t)(cw & 0xFF);
-        tr.board_bucket[p][0] = 0;
-        tr.board_bucket[p][1] = (uint8_t)(cw >> 8);
-        tr.board_bucket[p][2] = (uint8_t)(cw >> 16);
-        tr.board_bucket[p][3] = (uint8_t)(cw >> 24);
-      }
-      tr.payoff = u;
-      tr.reserved = 0;
+      if (n_act < 40) trace[t].actions[n_act] = (uint8_t)s;
     }
-    warp_add_counters(counters, 1u, n_visits, n_updates, 1u, (unsigned)N);
+    n_act++;
+    // pop the actor, apply (cfr_gpu.cu:803-807, 543-585)
+    q >>= 4;
+    nq--;
+    const int chips = chips_for(G, s, pot, pstack, to_call, cb, lfr);
+    abits = ((abits << 3) | (uint32_t)s) & 0x3FFFFFFFu;
+    path = path_step(path, s);
+    const int k = G.kind[s];
+    if (k == 0) {
+      folded |= 1u << player;
+    } else if (k != 1) {
+      const int nstack = pstack - chips, nbet = pbet + chips;
+      s_stack[player][tid] = (uint16_t)nstack;
+      s_bet[player][tid] = (uint16_t)nbet;
+      s_inv[player][tid] = (uint16_t)(s_inv[player][tid] + chips);
+      pot += chips;
+      if (nstack == 0) allin |= 1u << player;
+      if (nbet > cb) {
+        const int prev = cb;
+        const int rs = nbet - prev;
+        if (rs >= lfr || prev == 0) lfr = rs;
+        cb = nbet;
+        raises++;
+        q = 0;
+        nq = 0;
+        for (int i = 1; i < N; ++i) {
+          const int p = (player + i) % N;
+          if (!((folded >> p) & 1) && !((allin >> p) & 1)) q |= (uint32_t)p << (4 * nq++);
+        }
+      }
+    }
+    depth++;
   }
+
+  // Fold u into the recorded nodes' accumulators.
+  const long long fu = fix_r(u, rscale);
+  for (int i = 0; i < nrec; ++i) {
+    const uint32_t slot = s_rec_slot[i][tid];
+    const uint32_t sv = s_rec_sv[i][tid];
+    const int s = (int)(sv & 0xFF);
+    const uint32_t vm = sv >> 8;
+    const long long dsamp = fix_r(__fsub_rn(__fdiv_rn(u, s_rec_q[i][tid]), u), rscale);
+    if (touch_row(tv, slot, uid, vm)) {
+      atomicAdd(row_cnt(tv, slot), (1ull << 32) | 1ull);
+      atomicAdd(row_su(tv, slot), (unsigned long long)fu);
+      atomicAdd(row_da(tv, slot) + s, (unsigned long long)(dsamp + fu));
+    } else {
+      // Mask differs from the row's canonical one (an FNV slot shared by states
+      // with different legal actions): add every term directly.
+      atomicAdd(row_cnt(tv, slot), 1ull << 32);
+      float reg[kSlots], strat[kSlots];
+      load_regrets(tv, slot, reg);
+      node_strategy(reg, vm, strat);
+      long long dr[kSlots], dw[kSlots];
+#pragma unroll
+      for (int a = 0; a < kSlots; ++a) {
+        dr[a] = (a == s) ? dsamp : -fu;
+        dw[a] = fix_s(strat[a]);
+      }
+      add_direct(tv, slot, vm, dr, dw);
+    }
+  }
+  if (TRACE) {
+    mccfr_trace& tr = trace[t];
+    for (int i = 0; i < 12; ++i) tr.hole[i] = D.hole[i];
+    for (int i = 0; i < 5; ++i) tr.board[i] = D.board[i];
+    tr.dealer = (uint8_t)dealer;
+    tr.n_actions = (uint8_t)n_act;
+    tr.n_traverser_nodes = (uint8_t)nrec;
+    for (int p = 0; p < 6; ++p) {
+      const uint32_t cw = D.ctx[p];
+      tr.hole_bucket[p] = (uint8_t)(cw & 0xFF);
+      tr.board_bucket[p][0] = 0;
+      tr.board_bucket[p][1] = (uint8_t)(cw >> 8);
+      tr.board_bucket[p][2] = (uint8_t)(cw >> 16);
+      tr.board_bucket[p][3] = (uint8_t)(cw >> 24);
+    }
+    tr.payoff = u;
+    tr.reserved = 0;
+  }
+  warp_add_counters(counters, 1u, n_visits, n_updates, 1u, (unsigned)N);
 }
 
 }  // namespace mccfr
