@@ -234,6 +234,47 @@ int mccfr_eval7(mccfr_handle* h, const uint8_t* cards, uint16_t* ranks, size_t n
 int mccfr_eval7_device(mccfr_handle* h, const uint8_t* dev_cards,
                        uint16_t* dev_ranks, size_t n, float* ms);
 
+/* ---- batched form: many tables in one persistent kernel ------------------
+   No reference counterpart.  A batch groups existing handles
+   (tables), each with its own game, table and schedule; one iteration runs
+   phase p = 0..max players-1 as ONE persistent traversal launch over the
+   player-p updates of every table with more than p players, pulling
+   traversals from a device work queue, then one apply launch for those tables.
+   Each table's result is bit-identical to training it alone with the same
+   traversals per update.  All handles must be on one device, hold a rank
+   table, use external sampling, and not be used elsewhere while batched. */
+typedef struct mccfr_batch mccfr_batch;
+typedef struct mccfr_batch_tuning {
+  int32_t block;          /* threads per block: 64, 128 or 256 */
+  int32_t grab;           /* traversals each lane takes per work-queue grab: 1, 2, 4, 8 */
+  int32_t smem_frames;    /* frames of each walk's stack staged in shared memory: 0, 2, 4 */
+  int32_t probe_width;    /* table keys loaded per probe step: 1 or 2 */
+  int32_t reserved[4];
+} mccfr_batch_tuning;
+typedef struct mccfr_batch_stats {
+  int64_t iterations;
+  int64_t traversals;       /* all tables */
+  int64_t node_visits;
+  double traverse_ms;       /* CUDA-event time of the persistent traversal launches */
+  double total_ms;          /* CUDA-event time of whole iterations */
+  int32_t reserved[8];
+} mccfr_batch_stats;
+/* traversals[i] = traversals per player-update of tables[i]. */
+int mccfr_batch_create(mccfr_handle* const* tables, int n_tables, const int* traversals,
+                       mccfr_batch** out);
+void mccfr_batch_destroy(mccfr_batch* b);
+int mccfr_batch_set_tuning(mccfr_batch* b, const mccfr_batch_tuning* t);
+int mccfr_batch_get_tuning(mccfr_batch* b, mccfr_batch_tuning* t);
+/* Runs `iters` iterations of every table (one CUDA graph per iteration).
+   flags bit 1: time every iteration with CUDA events (synchronises per iteration). */
+int mccfr_batch_train(mccfr_batch* b, long long iters, int flags);
+/* Trains one real iteration per candidate tuning (results do not depend on the
+   tuning) and keeps the fastest; *best receives it.  Candidates: block x grab x
+   smem_frames x probe_width from the sets above, limited to `max_candidates`
+   (0 = all 72). */
+int mccfr_batch_autotune(mccfr_batch* b, int max_candidates, mccfr_batch_tuning* best);
+int mccfr_batch_get_stats(mccfr_batch* b, mccfr_batch_stats* out);
+
 /* ---- evaluation without device allocation --------------------------------
    No counterpart in the reference.  For callers that cannot allocate device
    memory (code inside a framework that owns every device allocation, or a

@@ -21,7 +21,7 @@ ORACLE_DIR = ROOT / "oracle"
 REFERENCE_SRC = Path("/root/reference/poker_cuda/src")
 
 SOURCES = ["mccfr.cu", "eval_static.cu", "handtable.cpp", "abstraction.cpp"]
-HEADERS = ["game.cuh", "table.cuh", "traverse_ref.cuh", "traverse_es.cuh", "handtable.h"]
+HEADERS = ["game.cuh", "table.cuh", "traverse_ref.cuh", "traverse_es.cuh", "batched.cuh", "handtable.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -29,6 +29,7 @@
 #include "table.cuh"
 #include "traverse_ref.cuh"
 #include "traverse_es.cuh"
+#include "batched.cuh"
 
 namespace mccfr {
 void build_preflop_lut(int mode, int buckets, uint8_t* lut);
@@ -44,30 +45,21 @@ namespace {
 
 constexpr int kRefBlock = 128;
 
-__global__ void k_advance(Sched* s, int N) {
-  int p = s->player + 1;
-  if (p >= N) {
-    p = 0;
-    s->iteration += 1;
-  }
-  s->player = p;
-}
-
 // Folds one player-update's accumulators into the rows it touched and zeroes
 // them (the sparse equivalent of kernel_clamp_regrets, cfr_gpu.cu:1018-1022).
 // Eight lanes per row, lane a owning action slot a: each row field is read and
 // written as one coalesced vector, and the row's regret matching gathers the
 // eight regrets with shuffles and sums them in slot order, like node_strategy.
-__global__ void __launch_bounds__(256) k_apply(const GameParams G, const TableView tv,
-                                               const Sched* __restrict__ sched, double rinv) {
+// `group`/`ngroups` enumerate the 8-lane groups working on this table.
+__device__ __forceinline__ void apply_rows(const GameParams& G, const TableView& tv, const Sched* sched, double rinv,
+                                           unsigned group, unsigned ngroups, bool leader) {
   const uint32_t uid = update_id(sched, G.N);
   const unsigned n = tv.n_touched[uid & 1];
   const double w = G.lcfr ? (double)(float)sched->iteration : 1.0;
   const double s32 = 2.3283064365386962890625e-10;  // 2^-32
   const int a = threadIdx.x & 7;
   const unsigned gmask = 0xFFu << (threadIdx.x & 24);
-  const unsigned ngroups = (gridDim.x * blockDim.x) >> 3;
-  for (unsigned i = (blockIdx.x * blockDim.x + threadIdx.x) >> 3; i < n; i += ngroups) {
+  for (unsigned i = group; i < n; i += ngroups) {
     const unsigned long long slot = tv.touched[i];
     const uint32_t m = (uint32_t)(*row_tag(tv, slot) & 0xFF);
     const unsigned long long cnt = *row_cnt(tv, slot);
@@ -107,7 +99,42 @@ __global__ void __launch_bounds__(256) k_apply(const GameParams G, const TableVi
       *row_flags(tv, slot) = 0;
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) tv.n_touched[(uid + 1) & 1] = 0;
+  if (leader) tv.n_touched[(uid + 1) & 1] = 0;
+}
+
+__global__ void __launch_bounds__(256) k_apply(const GameParams G, const TableView tv,
+                                               const Sched* __restrict__ sched, double rinv) {
+  apply_rows(G, tv, sched, rinv, (blockIdx.x * blockDim.x + threadIdx.x) >> 3, (gridDim.x * blockDim.x) >> 3,
+             blockIdx.x == 0 && threadIdx.x == 0);
+}
+
+// Apply of every table in a phase: blockIdx.y selects the table.
+__global__ void __launch_bounds__(256) k_apply_batched(const TableDesc* __restrict__ tables,
+                                                       const PhaseDesc* __restrict__ phase) {
+  const TableDesc& D = tables[phase->table[blockIdx.y]];
+  apply_rows(D.G, D.tv, D.sched, D.rinv, (blockIdx.x * blockDim.x + threadIdx.x) >> 3,
+             (gridDim.x * blockDim.x) >> 3, blockIdx.x == 0 && threadIdx.x == 0);
+}
+
+__global__ void k_advance(Sched* s, int N) {
+  int p = s->player + 1;
+  if (p >= N) {
+    p = 0;
+    s->iteration += 1;
+  }
+  s->player = p;
+}
+
+__global__ void k_advance_batched(const TableDesc* __restrict__ tables, const PhaseDesc* __restrict__ phase) {
+  const int j = threadIdx.x;
+  if (j >= phase->n) return;
+  const TableDesc& D = tables[phase->table[j]];
+  int p = D.sched->player + 1;
+  if (p >= D.G.N) {
+    p = 0;
+    D.sched->iteration += 1;
+  }
+  D.sched->player = p;
 }
 
 __global__ void k_export(const TableView tv, unsigned long long cap_slots,
@@ -1207,6 +1234,341 @@ int mccfr_eval7(mccfr_handle* h, const uint8_t* cards, uint16_t* ranks, size_t n
   cudaFree(dc);
   cudaFree(dr);
   return rc;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched form: many tables in one persistent kernel.
+// ---------------------------------------------------------------------------
+struct mccfr_batch {
+  std::vector<mccfr_handle*> tables;
+  std::vector<int> traversals;
+  int device = 0;
+  int max_players = 0;
+  cudaStream_t stream = nullptr;
+  TableDesc* d_tables = nullptr;
+  PhaseDesc* d_phases = nullptr;
+  std::vector<PhaseDesc> phases;
+  DealRec* d_deals = nullptr;
+  unsigned long long* d_work = nullptr;
+  unsigned long long max_items = 0;
+  mccfr_batch_tuning tuning{128, 2, 0, 1, {0, 0, 0, 0}};
+  cudaGraphExec_t graph = nullptr;
+  cudaEvent_t ev_it[2] = {nullptr, nullptr};
+  cudaEvent_t ev_ph[2 * MCCFR_MAX_PLAYERS] = {};
+  long long iterations = 0;
+  double traverse_ms = 0, total_ms = 0;
+  std::string last_error;
+};
+
+namespace {
+
+int bfail(mccfr_batch* b, int code, const char* msg) {
+  if (b) b->last_error = msg;
+  fprintf(stderr, "mccfr_batch: %s\n", msg);
+  return code;
+}
+
+#define BCK(call)                                                                        \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) return bfail(b, e_ == cudaErrorMemoryAllocation ? MCCFR_ERR_OOM : MCCFR_ERR_CUDA, \
+                                        cudaGetErrorString(e_));                          \
+  } while (0)
+
+using BatchedKernel = void (*)(const TableDesc*, const PhaseDesc*, const DealRec*, unsigned long long*, int);
+
+template <int B, int K, int W>
+BatchedKernel pick3() {
+  return k_traverse_batched<B, K, W>;
+}
+template <int B, int K>
+BatchedKernel pick2(int w) {
+  return w == 2 ? pick3<B, K, 2>() : pick3<B, K, 1>();
+}
+template <int B>
+BatchedKernel pick1(int k, int w) {
+  return k == 4 ? pick2<B, 4>(w) : k == 2 ? pick2<B, 2>(w) : pick2<B, 0>(w);
+}
+BatchedKernel pick_kernel(const mccfr_batch_tuning& t) {
+  return t.block == 64 ? pick1<64>(t.smem_frames, t.probe_width)
+         : t.block == 256 ? pick1<256>(t.smem_frames, t.probe_width)
+                          : pick1<128>(t.smem_frames, t.probe_width);
+}
+
+bool valid_tuning(const mccfr_batch_tuning& t) {
+  return (t.block == 64 || t.block == 128 || t.block == 256) && (t.grab == 1 || t.grab == 2 || t.grab == 4 || t.grab == 8) &&
+         (t.smem_frames == 0 || t.smem_frames == 2 || t.smem_frames == 4) && (t.probe_width == 1 || t.probe_width == 2);
+}
+
+size_t batched_smem(const mccfr_batch_tuning& t) {
+  return kBatchedHeadBytes + (size_t)t.smem_frames * t.block * sizeof(EsFrame);
+}
+
+// Enqueues one iteration: every phase's deal, persistent traversal, apply, advance.
+int batch_enqueue_iteration(mccfr_batch* b, bool capturing) {
+  const mccfr_batch_tuning& t = b->tuning;
+  BatchedKernel kern = pick_kernel(t);
+  const size_t smem = batched_smem(t);
+  BCK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, t.block, smem));
+  cudaDeviceProp prop;
+  BCK(cudaGetDeviceProperties(&prop, b->device));
+  const int grid = std::max(1, per_sm) * prop.multiProcessorCount;
+  const int32_t* T = b->tables[0]->d_hr;
+  auto rec = [&](cudaEvent_t e) {
+    return capturing ? cudaEventRecordWithFlags(e, b->stream, cudaEventRecordExternal) : cudaEventRecord(e, b->stream);
+  };
+  BCK(rec(b->ev_it[0]));
+  for (int p = 0; p < b->max_players; ++p) {
+    const PhaseDesc& P = b->phases[p];
+    const unsigned long long items = P.off[P.n];
+    BCK(cudaMemsetAsync(b->d_work + p, 0, sizeof(unsigned long long), b->stream));
+    const int dgrid = (int)std::min<unsigned long long>((items + 127) / 128, 148ull * 64);
+    k_deal_batched<<<std::max(1, dgrid), 128, 0, b->stream>>>(b->d_tables, b->d_phases + p, T, b->d_deals);
+    BCK(cudaGetLastError());
+    BCK(rec(b->ev_ph[2 * p]));
+    kern<<<grid, t.block, smem, b->stream>>>(b->d_tables, b->d_phases + p, b->d_deals, b->d_work + p, t.grab);
+    BCK(cudaGetLastError());
+    BCK(rec(b->ev_ph[2 * p + 1]));
+    k_apply_batched<<<dim3(148 * 2, P.n), 256, 0, b->stream>>>(b->d_tables, b->d_phases + p);
+    BCK(cudaGetLastError());
+    k_advance_batched<<<1, 64, 0, b->stream>>>(b->d_tables, b->d_phases + p);
+    BCK(cudaGetLastError());
+  }
+  BCK(rec(b->ev_it[1]));
+  return MCCFR_OK;
+}
+
+int batch_set_scheds(mccfr_batch* b) {
+  for (mccfr_handle* h : b->tables) {
+    h->h_sched->iteration = h->iterations_done + 1;
+    h->h_sched->player = 0;
+    h->h_sched->pad = 0;
+    BCK(cudaMemcpyAsync(h->d_sched, h->h_sched, sizeof(Sched), cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));  // pinned staging is reused by the next table
+  }
+  return MCCFR_OK;
+}
+
+int batch_after(mccfr_batch* b, long long iters) {
+  BCK(cudaStreamSynchronize(b->stream));
+  int worst = MCCFR_OK;
+  for (mccfr_handle* h : b->tables) {
+    h->iterations_done += iters;
+    h->launches += iters * h->cfg.num_players;
+    const int rc = check_device_error(h);
+    if (rc && !worst) worst = rc;
+  }
+  b->iterations += iters;
+  return worst;
+}
+
+void batch_time_phases(mccfr_batch* b) {
+  float ms = 0;
+  for (int p = 0; p < b->max_players; ++p)
+    if (cudaEventElapsedTime(&ms, b->ev_ph[2 * p], b->ev_ph[2 * p + 1]) == cudaSuccess) b->traverse_ms += ms;
+  if (cudaEventElapsedTime(&ms, b->ev_it[0], b->ev_it[1]) == cudaSuccess) b->total_ms += ms;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mccfr_batch_create(mccfr_handle* const* tables, int n, const int* traversals, mccfr_batch** out) {
+  if (!tables || !traversals || !out || n < 1 || n > kMaxBatchTables) return MCCFR_ERR_INVALID_ARG;
+  *out = nullptr;
+  mccfr_batch* b = new mccfr_batch();
+  auto bad = [&](int rc, const char* why) {
+    bfail(b, rc, why);
+    mccfr_batch_destroy(b);
+    return rc;
+  };
+  b->device = tables[0]->device;
+  for (int i = 0; i < n; ++i) {
+    mccfr_handle* h = tables[i];
+    if (!h || traversals[i] < 1) return bad(MCCFR_ERR_INVALID_ARG, "null table or traversal count < 1");
+    if (h->device != b->device) return bad(MCCFR_ERR_INVALID_ARG, "tables on different devices");
+    if (!h->has_table) return bad(MCCFR_ERR_NO_HAND_TABLE, "a table has no rank table loaded");
+    if (h->cfg.sampling != MCCFR_SAMPLING_EXTERNAL) return bad(MCCFR_ERR_INVALID_ARG, "batched tables use external sampling");
+    b->tables.push_back(h);
+    b->traversals.push_back(traversals[i]);
+    b->max_players = std::max(b->max_players, h->cfg.num_players);
+  }
+  if (cudaSetDevice(b->device) != cudaSuccess) return bad(MCCFR_ERR_CUDA, "cudaSetDevice");
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return bad(MCCFR_ERR_CUDA, "stream");
+  for (auto& e : b->ev_it)
+    if (cudaEventCreate(&e) != cudaSuccess) return bad(MCCFR_ERR_CUDA, "event");
+  for (auto& e : b->ev_ph)
+    if (cudaEventCreate(&e) != cudaSuccess) return bad(MCCFR_ERR_CUDA, "event");
+  std::vector<TableDesc> descs(n);
+  for (int i = 0; i < n; ++i) {
+    mccfr_handle* h = tables[i];
+    TableDesc& d = descs[i];
+    std::memset(&d, 0, sizeof(d));
+    d.G = h->gp;
+    d.tv = h->tv;
+    d.pre = h->d_pre;
+    d.cdf = h->d_cdf;
+    d.sched = h->d_sched;
+    d.counters = h->d_counters;
+    const int rb = regret_frac_bits(h->cfg, traversals[i]);
+    d.rscale = std::ldexp(1.0f, rb);
+    d.rinv = std::ldexp(1.0, -rb);
+    d.batch = traversals[i];
+  }
+  b->phases.resize(b->max_players);
+  for (int p = 0; p < b->max_players; ++p) {
+    PhaseDesc& P = b->phases[p];
+    std::memset(&P, 0, sizeof(P));
+    unsigned long long off = 0;
+    for (int i = 0; i < n; ++i) {
+      if (tables[i]->cfg.num_players <= p) continue;
+      P.table[P.n] = i;
+      P.off[P.n] = off;
+      off += (unsigned long long)traversals[i];
+      P.n++;
+    }
+    P.off[P.n] = off;
+    b->max_items = std::max(b->max_items, off);
+  }
+  if (cudaMalloc(&b->d_tables, n * sizeof(TableDesc)) != cudaSuccess ||
+      cudaMalloc(&b->d_phases, b->max_players * sizeof(PhaseDesc)) != cudaSuccess ||
+      cudaMalloc(&b->d_work, b->max_players * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&b->d_deals, b->max_items * sizeof(DealRec)) != cudaSuccess)
+    return bad(MCCFR_ERR_OOM, "batch buffers");
+  if (cudaMemcpy(b->d_tables, descs.data(), n * sizeof(TableDesc), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b->d_phases, b->phases.data(), b->max_players * sizeof(PhaseDesc), cudaMemcpyHostToDevice) !=
+          cudaSuccess)
+    return bad(MCCFR_ERR_CUDA, "batch upload");
+  *out = b;
+  return MCCFR_OK;
+}
+
+void mccfr_batch_destroy(mccfr_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  for (auto& e : b->ev_it)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : b->ev_ph)
+    if (e) cudaEventDestroy(e);
+  cudaFree(b->d_tables);
+  cudaFree(b->d_phases);
+  cudaFree(b->d_work);
+  cudaFree(b->d_deals);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+int mccfr_batch_set_tuning(mccfr_batch* b, const mccfr_batch_tuning* t) {
+  if (!b || !t || !valid_tuning(*t)) return MCCFR_ERR_INVALID_ARG;
+  b->tuning = *t;
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  return MCCFR_OK;
+}
+
+int mccfr_batch_get_tuning(mccfr_batch* b, mccfr_batch_tuning* t) {
+  if (!b || !t) return MCCFR_ERR_INVALID_ARG;
+  *t = b->tuning;
+  return MCCFR_OK;
+}
+
+int mccfr_batch_train(mccfr_batch* b, long long iters, int flags) {
+  if (!b || iters < 0) return MCCFR_ERR_INVALID_ARG;
+  if (iters == 0) return MCCFR_OK;
+  BCK(cudaSetDevice(b->device));
+  int rc = batch_set_scheds(b);
+  if (rc) return rc;
+  if (!b->graph) {
+    cudaGraph_t g = nullptr;
+    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    rc = batch_enqueue_iteration(b, true);
+    const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return bfail(b, MCCFR_ERR_CUDA, "batch graph capture");
+    const cudaError_t e2 = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e2 != cudaSuccess) return bfail(b, MCCFR_ERR_CUDA, "batch graph instantiate");
+  }
+  const bool timed = (flags & 2) != 0;
+  for (long long i = 0; i < iters; ++i) {
+    BCK(cudaGraphLaunch(b->graph, b->stream));
+    if (timed) {
+      BCK(cudaEventSynchronize(b->ev_it[1]));
+      batch_time_phases(b);
+    }
+  }
+  return batch_after(b, iters);
+}
+
+int mccfr_batch_autotune(mccfr_batch* b, int max_candidates, mccfr_batch_tuning* best) {
+  if (!b) return MCCFR_ERR_INVALID_ARG;
+  BCK(cudaSetDevice(b->device));
+  std::vector<mccfr_batch_tuning> cands;
+  for (int blk : {128, 64, 256})
+    for (int grab : {2, 1, 4, 8})
+      for (int k : {0, 2, 4})
+        for (int w : {1, 2}) cands.push_back(mccfr_batch_tuning{blk, grab, k, w, {0, 0, 0, 0}});
+  if (max_candidates > 0 && (int)cands.size() > max_candidates) cands.resize(max_candidates);
+  double best_ms = 1e300;
+  mccfr_batch_tuning best_t = b->tuning;
+  for (const mccfr_batch_tuning& t : cands) {
+    b->tuning = t;
+    int rc = batch_set_scheds(b);
+    if (rc) return rc;
+    rc = batch_enqueue_iteration(b, false);
+    if (rc) return rc;
+    BCK(cudaEventSynchronize(b->ev_it[1]));
+    float it_ms = 0;
+    double trav = 0;
+    for (int p = 0; p < b->max_players; ++p) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, b->ev_ph[2 * p], b->ev_ph[2 * p + 1]);
+      trav += ms;
+    }
+    cudaEventElapsedTime(&it_ms, b->ev_it[0], b->ev_it[1]);
+    b->traverse_ms += trav;
+    b->total_ms += it_ms;
+    rc = batch_after(b, 1);
+    if (rc) return rc;
+    if (trav < best_ms) {
+      best_ms = trav;
+      best_t = t;
+    }
+  }
+  b->tuning = best_t;
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  if (best) *best = best_t;
+  return MCCFR_OK;
+}
+
+int mccfr_batch_get_stats(mccfr_batch* b, mccfr_batch_stats* out) {
+  if (!b || !out) return MCCFR_ERR_INVALID_ARG;
+  std::memset(out, 0, sizeof(*out));
+  BCK(cudaSetDevice(b->device));
+  BCK(cudaStreamSynchronize(b->stream));
+  for (mccfr_handle* h : b->tables) {
+    Counters c;
+    BCK(cudaMemcpy(&c, h->d_counters, sizeof(c), cudaMemcpyDeviceToHost));
+    out->traversals += (int64_t)c.traversals;
+    out->node_visits += (int64_t)c.visits;
+  }
+  out->iterations = b->iterations;
+  out->traverse_ms = b->traverse_ms;
+  out->total_ms = b->total_ms;
+  return MCCFR_OK;
 }
 
 }  // extern "C"

@@ -79,29 +79,43 @@ __device__ __forceinline__ unsigned long long home_slot(const TableView& tv, uns
   return (key * 0x9E3779B97F4A7C15ull) >> (64 - tv.log2cap);
 }
 
-// Read-only lookup; returns the slot or -1.
+// Read-only lookup; returns the slot or -1.  W keys are loaded per probe step
+// (independent loads issued together); W is an autotuned probe width.
+template <int W = 1>
 __device__ __forceinline__ long long table_find(const TableView& tv, unsigned long long key) {
   unsigned long long s = home_slot(tv, key);
-  for (int step = 0; step < kProbeLimit; ++step) {
-    const unsigned long long k = __ldcg(row_key(tv, s));
-    if (k == key) return (long long)s;
-    if (k == 0) return -1;
-    s = (s + 1) & tv.mask;
+  for (int step = 0; step < kProbeLimit; step += W) {
+    unsigned long long k[W];
+#pragma unroll
+    for (int i = 0; i < W; ++i) k[i] = __ldcg(row_key(tv, (s + i) & tv.mask));
+#pragma unroll
+    for (int i = 0; i < W; ++i) {
+      if (k[i] == key) return (long long)((s + i) & tv.mask);
+      if (k[i] == 0) return -1;
+    }
+    s = (s + W) & tv.mask;
   }
   return -1;
 }
 
 // Find or insert; returns the slot, or -1 when the probe limit is exceeded.
+template <int W = 1>
 __device__ __forceinline__ long long table_insert(const TableView& tv, unsigned long long key) {
   unsigned long long s = home_slot(tv, key);
-  for (int step = 0; step < kProbeLimit; ++step) {
-    unsigned long long k = __ldcg(row_key(tv, s));
-    if (k == key) return (long long)s;
-    if (k == 0) {
-      k = atomicCAS(row_key(tv, s), 0ull, key);
-      if (k == 0 || k == key) return (long long)s;
+  for (int step = 0; step < kProbeLimit; step += W) {
+    unsigned long long k[W];
+#pragma unroll
+    for (int i = 0; i < W; ++i) k[i] = __ldcg(row_key(tv, (s + i) & tv.mask));
+#pragma unroll
+    for (int i = 0; i < W; ++i) {
+      const unsigned long long slot = (s + i) & tv.mask;
+      if (k[i] == key) return (long long)slot;
+      if (k[i] == 0) {
+        const unsigned long long prev = atomicCAS(row_key(tv, slot), 0ull, key);
+        if (prev == 0 || prev == key) return (long long)slot;
+      }
     }
-    s = (s + 1) & tv.mask;
+    s = (s + W) & tv.mask;
   }
   atomicOr(tv.err, kErrTableFull);
   return -1;

@@ -77,17 +77,30 @@ __device__ __forceinline__ void es_apply(const GameParams& G, EsState& s, int pl
   }
 }
 
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK)
-k_traverse_es(const GameParams G, const TableView tv, const DealRec* __restrict__ deals, const Sched* __restrict__ sched,
-              int batch, float rscale, Counters* __restrict__ counters) {
-  const uint32_t t = blockIdx.x * BLOCK + threadIdx.x;
-  if (t >= (uint32_t)batch) return;
-  const int up = sched->player;
-  const int N = G.N;
-  const uint32_t uid = update_id(sched, N);
+// Frame storage of one thread's walk: frames [0, K) in the caller's shared
+// memory (this thread's column, stride `stride` frames), deeper ones in local
+// memory.  K is an autotuned shared-memory stack depth.
+template <int K>
+struct FrameStack {
+  EsFrame* smem;
+  int stride;
+  EsFrame local[kMaxFrames - K];
+  __device__ __forceinline__ EsFrame& at(int i) {
+    if (K > 0 && i < K) return smem[i * stride];
+    return local[i - K];
+  }
+};
 
-  const DealRec& D = deals[t];
+struct EsCounts {
+  unsigned visits, updates, terminals;
+};
+
+// One external-sampling traversal (deal `D`, traversal index t, update uid of
+// player `up`): the updating player's subtree depth-first, opponents sampled.
+template <int W, class Frames>
+__device__ __forceinline__ void es_walk(const GameParams& G, const TableView& tv, const DealRec& D, uint32_t t,
+                                        uint32_t uid, int up, float rscale, Frames& fr, EsCounts& cnt) {
+  const int N = G.N;
   const int dealer = D.dealer;
   uint32_t ctx[kMaxPlayers], rank[kMaxPlayers];
 #pragma unroll
@@ -95,7 +108,6 @@ k_traverse_es(const GameParams G, const TableView tv, const DealRec* __restrict_
     ctx[p] = D.ctx[p];
     rank[p] = D.rank[p];
   }
-
   EsState cur;
   {
     for (int p = 0; p < kMaxPlayers; ++p) {
@@ -132,7 +144,6 @@ k_traverse_es(const GameParams G, const TableView tv, const DealRec* __restrict_
     }
   }
 
-  EsFrame fr[kMaxFrames];
   int sp = 0;
   unsigned n_visits = 0, n_updates = 0, n_term = 0;
   const uint32_t all_players = (1u << N) - 1;
@@ -185,7 +196,7 @@ k_traverse_es(const GameParams G, const TableView tv, const DealRec* __restrict_
       const uint32_t hb = cw & 0xFF;
       const uint32_t bkt = cur.street ? ((cw >> (8 * cur.street)) & 0xFF) : 0u;
       const unsigned long long key = info_key(G, player, hb, bkt, cur.street, cur.abits, cur.path);
-      const long long slot = table_insert(tv, key);
+      const long long slot = table_insert<W>(tv, key);
       float reg[kSlots];
       load_regrets(tv, slot, reg);
       n_visits++;
@@ -195,7 +206,7 @@ k_traverse_es(const GameParams G, const TableView tv, const DealRec* __restrict_
           aborted = true;
           break;
         }
-        EsFrame& F = fr[sp++];
+        EsFrame& F = fr.at(sp++);
         F.st = cur;
         node_strategy(reg, vm, F.strat);
         F.vh = 0.0f;
@@ -234,7 +245,7 @@ k_traverse_es(const GameParams G, const TableView tv, const DealRec* __restrict_
     // ---- return `value` to the frames
     bool resumed = false;
     while (sp > 0) {
-      EsFrame& F = fr[sp - 1];
+      EsFrame& F = fr.at(sp - 1);
       const int a = F.next_a;
       atomicAdd(row_da(tv, F.slot) + a, (unsigned long long)fix_r(value, rscale));
       F.vh = __fadd_rn(F.vh, __fmul_rn(F.strat[a], value));
@@ -266,14 +277,33 @@ k_traverse_es(const GameParams G, const TableView tv, const DealRec* __restrict_
     }
     if (!resumed) break;
   }
-  warp_add_counters(counters, 1u, n_visits, n_updates, n_term, (unsigned)N);
+  cnt.visits += n_visits;
+  cnt.updates += n_updates;
+  cnt.terminals += n_term;
+}
+
+template <int BLOCK, int K, int W>
+__global__ void __launch_bounds__(BLOCK)
+k_traverse_es(const GameParams G, const TableView tv, const DealRec* __restrict__ deals, const Sched* __restrict__ sched,
+              int batch, float rscale, Counters* __restrict__ counters) {
+  extern __shared__ EsFrame s_frames[];  // [K][BLOCK]
+  const uint32_t t = blockIdx.x * BLOCK + threadIdx.x;
+  if (t >= (uint32_t)batch) return;
+  const int up = sched->player;
+  const uint32_t uid = update_id(sched, G.N);
+  FrameStack<K> fr;
+  fr.smem = s_frames + threadIdx.x;
+  fr.stride = BLOCK;
+  EsCounts c{0, 0, 0};
+  es_walk<W>(G, tv, deals[t], t, uid, up, rscale, fr, c);
+  warp_add_counters(counters, 1u, c.visits, c.updates, c.terminals, (unsigned)G.N);
 }
 
 inline void launch_traverse_es(const GameParams& G, const TableView& tv, const DealRec* deals, const Sched* sched,
                                int batch, float rscale, Counters* counters, cudaStream_t stream) {
   constexpr int B = 128;
   const int grid = (batch + B - 1) / B;
-  k_traverse_es<B><<<grid, B, 0, stream>>>(G, tv, deals, sched, batch, rscale, counters);
+  k_traverse_es<B, 0, 1><<<grid, B, 0, stream>>>(G, tv, deals, sched, batch, rscale, counters);
 }
 
 }  // namespace mccfr

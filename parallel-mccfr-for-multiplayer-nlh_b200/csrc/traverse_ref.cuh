@@ -77,17 +77,12 @@ __device__ __forceinline__ uint32_t update_id(const Sched* s, int N) {
 }
 
 // Deal, buckets and river ranks of traversal t of update `uid`
-// (cfr_gpu.cu:460-470, 476-489, 942-952, 963).
-__global__ void __launch_bounds__(128) k_deal(const GameParams G, const HandView hv, const Sched* __restrict__ sched,
-                                              int batch, DealRec* __restrict__ out) {
-  __shared__ uint8_t s_pre[52 * 52];
-  for (int i = threadIdx.x; i < 52 * 52 / 4; i += blockDim.x)
-    reinterpret_cast<uint32_t*>(s_pre)[i] = __ldg(reinterpret_cast<const uint32_t*>(hv.pre) + i);
-  __syncthreads();
-  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (uint32_t)batch) return;
+// (cfr_gpu.cu:460-470, 476-489, 942-952, 963).  `pre` is the 52x52 preflop LUT
+// (shared or global memory), `cdf` the rank-CDF LUTs.
+__device__ __forceinline__ void deal_one(const GameParams& G, const int32_t* __restrict__ T, const uint8_t* pre,
+                                         const uint8_t* __restrict__ cdf, uint32_t t, uint32_t uid,
+                                         DealRec* __restrict__ out) {
   const int N = G.N;
-  const uint32_t uid = update_id(sched, N);
   const int n_deal = 2 * N + 5;
   uint32_t words[24];
   const int nblk = (n_deal + 1 + 3) / 4;
@@ -119,7 +114,6 @@ __global__ void __launch_bounds__(128) k_deal(const GameParams G, const HandView
 #pragma unroll
   for (int i = 0; i < 10; ++i) r.pad[i] = 0;
 
-  const int32_t* T = hv.hr;
   int32_t b = __ldg(T + 53 + to_rm(r.board[0]));
   b = __ldg(T + b + to_rm(r.board[1]));
   b = __ldg(T + b + to_rm(r.board[2]));
@@ -142,7 +136,7 @@ __global__ void __launch_bounds__(128) k_deal(const GameParams G, const HandView
     r.ctx[p] = 0;
     r.rank[p] = 0;
     if (p >= N) continue;
-    const uint32_t hb = s_pre[r.hole[2 * p] * 52 + r.hole[2 * p + 1]];
+    const uint32_t hb = pre[r.hole[2 * p] * 52 + r.hole[2 * p + 1]];
     const uint32_t rr = decode16((uint32_t)r7[p] & 0xFFFF);
     uint32_t b1, b2, b3;
     if (G.postflop_mode == 0) {
@@ -151,17 +145,28 @@ __global__ void __launch_bounds__(128) k_deal(const GameParams G, const HandView
       b2 = ref_linear_bucket(decode16((uint32_t)s6[p] & 0xFFFF), G.post_b[1]);
       b3 = ref_linear_bucket(rr, G.post_b[2]);
     } else {
-      b1 = __ldg(hv.cdf + decode16((uint32_t)__ldg(T + s5[p]) & 0xFFFF));
-      b2 = __ldg(hv.cdf + 7463 + decode16((uint32_t)__ldg(T + s6[p]) & 0xFFFF));
-      b3 = __ldg(hv.cdf + 2 * 7463 + rr);
+      b1 = __ldg(cdf + decode16((uint32_t)__ldg(T + s5[p]) & 0xFFFF));
+      b2 = __ldg(cdf + 7463 + decode16((uint32_t)__ldg(T + s6[p]) & 0xFFFF));
+      b3 = __ldg(cdf + 2 * 7463 + rr);
     }
     r.ctx[p] = hb | (b1 << 8) | (b2 << 16) | (b3 << 24);
     r.rank[p] = (uint16_t)rr;
   }
   const uint4* src = reinterpret_cast<const uint4*>(&r);
-  uint4* dst = reinterpret_cast<uint4*>(out + t);
+  uint4* dst = reinterpret_cast<uint4*>(out);
 #pragma unroll
   for (int i = 0; i < 4; ++i) dst[i] = src[i];
+}
+
+__global__ void __launch_bounds__(128) k_deal(const GameParams G, const HandView hv, const Sched* __restrict__ sched,
+                                              int batch, DealRec* __restrict__ out) {
+  __shared__ uint8_t s_pre[52 * 52];
+  for (int i = threadIdx.x; i < 52 * 52 / 4; i += blockDim.x)
+    reinterpret_cast<uint32_t*>(s_pre)[i] = __ldg(reinterpret_cast<const uint32_t*>(hv.pre) + i);
+  __syncthreads();
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (uint32_t)batch) return;
+  deal_one(G, hv.hr, s_pre, hv.cdf, t, update_id(sched, G.N), out + t);
 }
 
 // Side-pot showdown for player `up` (cfr_gpu.cu:694-753).  The distinct non-zero

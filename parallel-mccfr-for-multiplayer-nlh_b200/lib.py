@@ -66,6 +66,20 @@ class Stats(Structure):
     ]
 
 
+class BatchTuning(Structure):
+    _fields_ = [("block", c_int32), ("grab", c_int32), ("smem_frames", c_int32), ("probe_width", c_int32),
+                ("reserved", c_int32 * 4)]
+
+    def as_dict(self) -> dict:
+        return {"block": self.block, "grab": self.grab, "smem_frames": self.smem_frames,
+                "probe_width": self.probe_width}
+
+
+class BatchStats(Structure):
+    _fields_ = [("iterations", c_int64), ("traversals", c_int64), ("node_visits", c_int64),
+                ("traverse_ms", c_double), ("total_ms", c_double), ("reserved", c_int32 * 8)]
+
+
 class Trace(Structure):
     _fields_ = [
         ("hole", c_uint8 * 12), ("board", c_uint8 * 5), ("dealer", c_uint8), ("n_actions", c_uint8),
@@ -110,6 +124,13 @@ SIGNATURES = {
     "mccfr_eval7": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),
     "mccfr_eval7_device": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t, POINTER(c_float)]),
     "mccfr_eval7_static": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),
+    "mccfr_batch_create": (c_int, [c_void_p, c_int, c_void_p, POINTER(c_void_p)]),
+    "mccfr_batch_destroy": (None, [c_void_p]),
+    "mccfr_batch_set_tuning": (c_int, [c_void_p, c_void_p]),
+    "mccfr_batch_get_tuning": (c_int, [c_void_p, c_void_p]),
+    "mccfr_batch_train": (c_int, [c_void_p, c_longlong, c_int]),
+    "mccfr_batch_autotune": (c_int, [c_void_p, c_int, c_void_p]),
+    "mccfr_batch_get_stats": (c_int, [c_void_p, c_void_p]),
 }
 EVAL7_STATIC_MAX_HANDS = 1 << 18
 

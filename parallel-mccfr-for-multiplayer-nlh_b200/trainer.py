@@ -166,3 +166,61 @@ class GPUCFRTrainer:
         out = np.empty(c.shape[0], dtype=np.uint16)
         L.check(self._lib.mccfr_eval7(self._h, L.ptr(c), L.ptr(out), c.shape[0]), self._h)
         return out
+
+
+class Batch:
+    """Several trainers (tables) trained together by one persistent kernel per
+    phase; each table's result equals training it alone (mccfr_batch_*)."""
+
+    def __init__(self, trainers: list, traversals: list[int]):
+        self._lib = L.load()
+        self.trainers = list(trainers)  # keep the handles alive
+        arr = (ctypes.c_void_p * len(trainers))(*[t.handle.value for t in trainers])
+        cnt = (ctypes.c_int * len(traversals))(*[int(x) for x in traversals])
+        b = c_void_p()
+        rc = self._lib.mccfr_batch_create(arr, len(trainers), cnt, byref(b))
+        L.check(rc)
+        self._b = b
+
+    def close(self) -> None:
+        if getattr(self, "_b", None):
+            self._lib.mccfr_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def train(self, iters: int, timed: bool = False) -> None:
+        L.check(self._lib.mccfr_batch_train(self._b, int(iters), 2 if timed else 0))
+        for t in self.trainers:
+            t.iterations_done += int(iters)
+
+    def autotune(self, max_candidates: int = 0) -> dict:
+        best = L.BatchTuning()
+        L.check(self._lib.mccfr_batch_autotune(self._b, int(max_candidates), byref(best)))
+        n = len(self.candidates(max_candidates))
+        for t in self.trainers:
+            t.iterations_done += n
+        return best.as_dict()
+
+    @staticmethod
+    def candidates(max_candidates: int = 0) -> list:
+        c = [(b, g, k, w) for b in (128, 64, 256) for g in (2, 1, 4, 8) for k in (0, 2, 4) for w in (1, 2)]
+        return c[:max_candidates] if max_candidates > 0 else c
+
+    def set_tuning(self, block=128, grab=2, smem_frames=0, probe_width=1) -> None:
+        t = L.BatchTuning(block, grab, smem_frames, probe_width)
+        L.check(self._lib.mccfr_batch_set_tuning(self._b, byref(t)))
+
+    def tuning(self) -> dict:
+        t = L.BatchTuning()
+        L.check(self._lib.mccfr_batch_get_tuning(self._b, byref(t)))
+        return t.as_dict()
+
+    def stats(self) -> L.BatchStats:
+        s = L.BatchStats()
+        L.check(self._lib.mccfr_batch_get_stats(self._b, byref(s)))
+        return s

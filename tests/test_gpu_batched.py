@@ -1,0 +1,75 @@
+"""The batched persistent form against the plain trainer: every table of a
+batch ends bit-identical to the same table trained alone, whatever the tuning."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import mccfr
+
+L = mccfr.lib
+pytestmark = pytest.mark.gpu
+
+
+def small_tables():
+    """Three uneven tables: heads-up 20BB, 6-max 100BB, and 3-handed 50BB with 3 actions."""
+    hu = L.preset(L.PRESET_HU_20BB)
+    six = L.preset(L.PRESET_6MAX_100BB)
+    three = L.preset(L.PRESET_HU_20BB)
+    three.num_players = 3
+    three.starting_stack = 5000
+    three.num_actions = 3
+    three.action_kind[2] = L.ACT_ALL_IN
+    three.seed = 7
+    out = []
+    for c in (hu, six, three):
+        c.table_log2 = 22
+        c.key_bits = 21
+        out.append(c)
+    return out, [3000, 200, 1500]
+
+
+def make(cfgs, table):
+    ts = []
+    for c in cfgs:
+        t = mccfr.GPUCFRTrainer(config=c)
+        t.set_hand_table(table)
+        ts.append(t)
+    return ts
+
+
+def rows_equal(a, b):
+    for f in ("keys", "visits", "regrets", "strategy_sum"):
+        assert np.array_equal(np.asarray(a[f]).view(np.uint8), np.asarray(b[f]).view(np.uint8)), f
+
+
+def test_batched_equals_plain(hand_table):
+    cfgs, trav = small_tables()
+    plain = make(cfgs, hand_table)
+    for t, n in zip(plain, trav):
+        t.train(2, n, verbose=False)
+    batched = make(cfgs, hand_table)
+    b = mccfr.Batch(batched, trav)
+    b.train(2)
+    for p, q in zip(plain, batched):
+        rows_equal(p.export_rows(), q.export_rows())
+    st = b.stats()
+    assert st.iterations == 2
+    assert st.traversals == sum(2 * n * c.num_players for n, c in zip(trav, cfgs))
+    b.close()
+
+
+def test_autotune_keeps_results(hand_table):
+    cfgs, trav = small_tables()
+    plain = make(cfgs, hand_table)
+    batched = make(cfgs, hand_table)
+    b = mccfr.Batch(batched, trav)
+    best = b.autotune(max_candidates=6)  # 6 real iterations, one per tuning
+    assert best in [dict(block=x, grab=g, smem_frames=k, probe_width=w) for x, g, k, w in mccfr.Batch.candidates(6)]
+    b.set_tuning(block=64, grab=4, smem_frames=2, probe_width=2)
+    b.train(1)
+    for t, n in zip(plain, trav):
+        t.train(7, n, verbose=False)
+    for p, q in zip(plain, batched):
+        rows_equal(p.export_rows(), q.export_rows())
+    b.close()
