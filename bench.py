@@ -168,6 +168,109 @@ def cpu_traversal_rate(L, cfg, batch_sample: int, reps: int = 1) -> tuple[float,
     return batch_sample * reps / dt, {"cores": threads, "seconds": dt}
 
 
+def batched_same_table(m, L, table, args, plain_value) -> dict:
+    """The headline 6-max table trained through the batched persistent form:
+    autotuned on real iterations, then timed like the headline."""
+    import torch
+
+    cfg, batch = make_config(L, args.workload)
+    if args.batch:
+        batch = args.batch
+    t = m.GPUCFRTrainer(config=cfg)
+    t.set_hand_table(table)
+    b = m.Batch([t], [batch])
+    best = b.autotune(max_candidates=16)
+    b.train(args.warmup)
+    s0 = b.stats()
+    b.train(args.steps, timed=True)
+    s1 = b.stats()
+    n = s1.traversals - s0.traversals
+    ms = s1.total_ms - s0.total_ms
+    b.close()
+    t.close()
+    v = n / (ms / 1e3)
+    return {"traversals_per_s": v, "vs_plain": v / plain_value, "tuning": best, "iterations": args.steps,
+            "traverse_ms_per_iteration": (s1.traverse_ms - s0.traverse_ms) / args.steps,
+            "note": "same table, seed and traversals per update as the headline; results are bit-identical "
+                    "to plain training (tests/test_gpu_batched.py)"}
+
+
+ACTION_SETS = {
+    3: [(0, 0, 1), (3, 0, 1), (6, 0, 1)],
+    4: [(0, 0, 1), (3, 0, 1), (5, 1, 1), (6, 0, 1)],
+    5: [(0, 0, 1), (3, 0, 1), (5, 1, 2), (5, 1, 1), (6, 0, 1)],
+    6: [(0, 0, 1), (3, 0, 1), (5, 1, 2), (5, 1, 1), (5, 2, 1), (6, 0, 1)],
+}
+
+
+def multitable_configs(L, n_tables=64, seed=2, scale=16):
+    """Uneven tables: players U{2..6}, stacks U[10,200] BB, 3-6 actions, traversals
+    per update round(LogNormal(14, 1)) / scale."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_tables):
+        c = L.preset(L.PRESET_HU_20BB)
+        c.num_players = int(rng.integers(2, 7))
+        c.starting_stack = int(rng.integers(10, 201)) * c.big_blind
+        na = int(rng.choice([3, 4, 5, 6]))
+        c.num_actions = na
+        for a, (k, num, den) in enumerate(ACTION_SETS[na]):
+            c.action_kind[a], c.action_num[a], c.action_den[a] = k, num, den
+        c.raise_cap = 3
+        c.table_log2 = 22
+        c.key_bits = 21
+        c.seed = 1000 + i
+        n = max(1024, int(round(rng.lognormal(14.0, 1.0) / scale)))
+        out.append((c, n))
+    return out
+
+
+def multitable(m, L, table, iters=2) -> dict:
+    import torch
+
+    specs = multitable_configs(L)
+    def make():
+        ts = []
+        for c, _ in specs:
+            t = m.GPUCFRTrainer(config=c)
+            t.set_hand_table(table)
+            ts.append(t)
+        return ts
+    # plain: each table's iteration on its own, one after another
+    plain = make()
+    for t, (c, n) in zip(plain, specs):
+        t.train(1, n, verbose=False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(iters):
+        for t, (c, n) in zip(plain, specs):
+            t.train(1, n, verbose=False)
+    torch.cuda.synchronize()
+    plain_s = time.perf_counter() - t0
+    for t in plain:
+        t.close()
+    batched = make()
+    b = m.Batch(batched, [n for _, n in specs])
+    best = b.autotune(max_candidates=16)
+    b.train(1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.train(iters)
+    torch.cuda.synchronize()
+    batched_s = time.perf_counter() - t0
+    b.close()
+    for t in batched:
+        t.close()
+    trav = iters * sum(n * c.num_players for c, n in specs)
+    return {"tables": len(specs), "traversals_per_iteration": trav // iters,
+            "plain_traversals_per_s": trav / plain_s, "batched_traversals_per_s": trav / batched_s,
+            "speedup": plain_s / batched_s, "tuning": best,
+            "workload": "64 tables, players U{2..6}, stacks U[10,200]BB, 3-6 actions, traversals/update "
+                        "LogNormal(14,1)/16, seed 2; wall clock over 2 iterations after warm-up"}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -303,8 +406,11 @@ def main():
         "node_visits_per_s": visits / (ms / 1e3) * world,
     }
 
+    tr.close()
     if rank == 0 and world == 1 and not args.no_extras:
         extras = {}
+        extras["batched_same_table"] = batched_same_table(m, L, table, args, value)
+        extras["c3_multitable"] = multitable(m, L, table)
         for wl in ("ref8-6max", "6max-100bb-refrule"):
             if wl == args.workload:
                 continue
@@ -334,7 +440,6 @@ def main():
         out["cpu_baseline"] = {"value": rate, "unit": "traversals/s", "cores": info["cores"], "kind": "port",
                                "sample": f"{sample} traversals of one player-update (iteration 1, player 0), "
                                          f"{info['seconds']:.1f} s on {info['cores']} threads"}
-    tr.close()
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:

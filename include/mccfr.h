@@ -249,7 +249,9 @@ typedef struct mccfr_batch_tuning {
   int32_t grab;           /* traversals each lane takes per work-queue grab: 1, 2, 4, 8 */
   int32_t smem_frames;    /* frames of each walk's stack staged in shared memory: 0, 2, 4 */
   int32_t probe_width;    /* table keys loaded per probe step: 1 or 2 */
-  int32_t reserved[4];
+  int32_t warp_sync;      /* 1: a warp takes 32 traversals at once and starts them together;
+                             0: each lane takes its next traversal as soon as it is idle */
+  int32_t reserved[3];
 } mccfr_batch_tuning;
 typedef struct mccfr_batch_stats {
   int64_t iterations;
@@ -269,9 +271,10 @@ int mccfr_batch_get_tuning(mccfr_batch* b, mccfr_batch_tuning* t);
    flags bit 1: time every iteration with CUDA events (synchronises per iteration). */
 int mccfr_batch_train(mccfr_batch* b, long long iters, int flags);
 /* Trains one real iteration per candidate tuning (results do not depend on the
-   tuning) and keeps the fastest; *best receives it.  Candidates: block x grab x
-   smem_frames x probe_width from the sets above, limited to `max_candidates`
-   (0 = all 72). */
+   tuning) and keeps the one with the least traversal-kernel time per node
+   visit; *best receives it.  Candidates: block x grab x
+   smem_frames x warp_sync x probe_width from the sets above, limited to the
+   first `max_candidates` (0 = all 144). */
 int mccfr_batch_autotune(mccfr_batch* b, int max_candidates, mccfr_batch_tuning* best);
 int mccfr_batch_get_stats(mccfr_batch* b, mccfr_batch_stats* out);
 

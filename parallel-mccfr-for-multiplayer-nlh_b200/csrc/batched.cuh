@@ -70,58 +70,92 @@ __global__ void __launch_bounds__(128) k_deal_batched(const TableDesc* __restric
   }
 }
 
-// Bytes of dynamic shared memory before the frame area: the phase descriptor
-// and the descriptors of the phase's tables.
-constexpr size_t kBatchedHeadBytes =
-    ((sizeof(PhaseDesc) + 15) / 16) * 16 + ((kMaxBatchTables * sizeof(TableDesc) + 15) / 16) * 16;
+// A phase's descriptors passed by value: they live in the kernel's parameter
+// space and are read through the constant cache, like the plain kernel's game
+// parameters (a warp mostly works on one table, so the reads are uniform).
+struct PhaseParams {
+  unsigned long long off[kMaxBatchTables + 1];
+  int n;
+  int pad;
+  TableDesc T[kMaxBatchTables];  // the phase's tables, in phase order
+};
 
-// Persistent external-sampling traversal over a phase's items.  Each warp takes
-// `grab` items per lane at a time from `work`.
-template <int BLOCK, int K, int W>
-__global__ void __launch_bounds__(BLOCK)
-k_traverse_batched(const TableDesc* __restrict__ tables, const PhaseDesc* __restrict__ phase,
-                   const DealRec* __restrict__ deals, unsigned long long* __restrict__ work, int grab) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  PhaseDesc& P = *reinterpret_cast<PhaseDesc*>(smem_raw);
-  TableDesc* s_tab = reinterpret_cast<TableDesc*>(smem_raw + ((sizeof(PhaseDesc) + 15) / 16) * 16);
-  EsFrame* s_frames = reinterpret_cast<EsFrame*>(smem_raw + kBatchedHeadBytes);
-  for (int i = threadIdx.x; i < (int)(sizeof(PhaseDesc) / 4); i += BLOCK)
-    reinterpret_cast<uint32_t*>(&P)[i] = reinterpret_cast<const uint32_t*>(phase)[i];
-  __syncthreads();
-  // descriptors of this phase's tables, in phase order
-  for (int i = threadIdx.x; i < P.n * (int)(sizeof(TableDesc) / 4); i += BLOCK) {
-    const int j = i / (int)(sizeof(TableDesc) / 4), w = i % (int)(sizeof(TableDesc) / 4);
-    reinterpret_cast<uint32_t*>(s_tab + j)[w] = reinterpret_cast<const uint32_t*>(tables + P.table[j])[w];
+__device__ __forceinline__ int param_table_of(const PhaseParams& P, unsigned long long g) {
+  int lo = 0, hi = P.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (P.off[mid] <= g) lo = mid;
+    else hi = mid - 1;
   }
-  __syncthreads();
+  return lo;
+}
+
+// Persistent external-sampling traversal over a phase's items.  Each lane takes
+// its next `grab` consecutive items from `work` as soon as it is idle (lanes
+// that become idle together share one atomic), so no lane waits for the rest of
+// its warp.  Counters are summed per lane while it stays on one table.
+template <int BLOCK, int K, int W>
+__global__ void __launch_bounds__(BLOCK, 2048 / BLOCK / 2)
+k_traverse_batched(const __grid_constant__ PhaseParams P, const DealRec* __restrict__ deals,
+                   unsigned long long* __restrict__ work, int grab, int warp_sync) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  EsFrame* s_frames = reinterpret_cast<EsFrame*>(smem_raw);
   const unsigned long long total = P.off[P.n];
-  const int lane = threadIdx.x & 31;
   FrameStack<K> fr;
   fr.smem = s_frames + threadIdx.x;
   fr.stride = BLOCK;
+  int cur_j = -1;
+  unsigned long long c_trav = 0, c_vis = 0, c_upd = 0, c_term = 0;
+  auto flush = [&]() {
+    if (cur_j >= 0 && c_trav) {
+      Counters* cn = P.T[cur_j].counters;
+      atomicAdd(&cn->traversals, c_trav);
+      atomicAdd(&cn->visits, c_vis);
+      atomicAdd(&cn->updates, c_upd);
+      atomicAdd(&cn->terminals, c_term);
+      atomicAdd(&cn->evals, c_trav * (unsigned long long)P.T[cur_j].G.N);
+    }
+    c_trav = c_vis = c_upd = c_term = 0;
+  };
+  const int lane = threadIdx.x & 31;
   for (;;) {
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(work, 32ull * (unsigned long long)grab);
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (base >= total) break;
+    unsigned long long base = 0, stride = 1;
+    if (warp_sync) {
+      // the whole warp takes 32*grab items and starts them together
+      if (lane == 0) base = atomicAdd(work, 32ull * grab);
+      base = __shfl_sync(0xFFFFFFFFu, base, 0) + lane;
+      stride = 32;
+      if (base - lane >= total) break;
+    } else {
+      // idle lanes that arrive together take consecutive chunks with one atomic
+      const unsigned act = __activemask();
+      const int leader = __ffs(act) - 1;
+      const int rank = __popc(act & ((1u << lane) - 1));
+      if (lane == leader) base = atomicAdd(work, (unsigned long long)__popc(act) * grab);
+      base = __shfl_sync(act, base, leader) + (unsigned long long)rank * grab;
+      if (base >= total) break;
+    }
     for (int k = 0; k < grab; ++k) {
-      const unsigned long long g = base + (unsigned long long)k * 32 + lane;
+      const unsigned long long g = base + k * stride;
       if (g >= total) break;
-      const int j = phase_table_of(P, g);
-      const TableDesc& D = s_tab[j];
+      const int j = param_table_of(P, g);
+      if (j != cur_j) {
+        flush();
+        cur_j = j;
+      }
+      const TableDesc& D = P.T[j];
       const uint32_t t = (uint32_t)(g - P.off[j]);
       const Sched* sc = D.sched;
       EsCounts c{0, 0, 0};
       es_walk<W>(D.G, D.tv, deals[g], t, update_id(sc, D.G.N), sc->player, D.rscale, fr, c);
-      Counters* cn = D.counters;
-      atomicAdd(&cn->traversals, 1ull);
-      atomicAdd(&cn->visits, (unsigned long long)c.visits);
-      atomicAdd(&cn->updates, (unsigned long long)c.updates);
-      atomicAdd(&cn->terminals, (unsigned long long)c.terminals);
-      atomicAdd(&cn->evals, (unsigned long long)D.G.N);
+      c_trav++;
+      c_vis += c.visits;
+      c_upd += c.updates;
+      c_term += c.terminals;
     }
-    __syncwarp();
+    if (warp_sync) __syncwarp();
   }
+  flush();
 }
 
 }  // namespace mccfr

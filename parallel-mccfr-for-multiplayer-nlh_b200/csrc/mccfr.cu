@@ -1250,10 +1250,11 @@ struct mccfr_batch {
   TableDesc* d_tables = nullptr;
   PhaseDesc* d_phases = nullptr;
   std::vector<PhaseDesc> phases;
+  std::vector<PhaseParams> params;  // by-value descriptors of each phase's traversal launch
   DealRec* d_deals = nullptr;
   unsigned long long* d_work = nullptr;
   unsigned long long max_items = 0;
-  mccfr_batch_tuning tuning{128, 2, 0, 1, {0, 0, 0, 0}};
+  mccfr_batch_tuning tuning{128, 2, 0, 1, 1, {0, 0, 0}};
   cudaGraphExec_t graph = nullptr;
   cudaEvent_t ev_it[2] = {nullptr, nullptr};
   cudaEvent_t ev_ph[2 * MCCFR_MAX_PLAYERS] = {};
@@ -1277,7 +1278,7 @@ int bfail(mccfr_batch* b, int code, const char* msg) {
                                         cudaGetErrorString(e_));                          \
   } while (0)
 
-using BatchedKernel = void (*)(const TableDesc*, const PhaseDesc*, const DealRec*, unsigned long long*, int);
+using BatchedKernel = void (*)(const PhaseParams, const DealRec*, unsigned long long*, int, int);
 
 template <int B, int K, int W>
 BatchedKernel pick3() {
@@ -1299,11 +1300,12 @@ BatchedKernel pick_kernel(const mccfr_batch_tuning& t) {
 
 bool valid_tuning(const mccfr_batch_tuning& t) {
   return (t.block == 64 || t.block == 128 || t.block == 256) && (t.grab == 1 || t.grab == 2 || t.grab == 4 || t.grab == 8) &&
-         (t.smem_frames == 0 || t.smem_frames == 2 || t.smem_frames == 4) && (t.probe_width == 1 || t.probe_width == 2);
+         (t.smem_frames == 0 || t.smem_frames == 2 || t.smem_frames == 4) && (t.probe_width == 1 || t.probe_width == 2) &&
+         (t.warp_sync == 0 || t.warp_sync == 1);
 }
 
 size_t batched_smem(const mccfr_batch_tuning& t) {
-  return kBatchedHeadBytes + (size_t)t.smem_frames * t.block * sizeof(EsFrame);
+  return (size_t)t.smem_frames * t.block * sizeof(EsFrame);
 }
 
 // Enqueues one iteration: every phase's deal, persistent traversal, apply, advance.
@@ -1312,6 +1314,8 @@ int batch_enqueue_iteration(mccfr_batch* b, bool capturing) {
   BatchedKernel kern = pick_kernel(t);
   const size_t smem = batched_smem(t);
   BCK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  BCK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           t.smem_frames ? (int)cudaSharedmemCarveoutDefault : 0));
   int per_sm = 0;
   BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, t.block, smem));
   cudaDeviceProp prop;
@@ -1330,7 +1334,7 @@ int batch_enqueue_iteration(mccfr_batch* b, bool capturing) {
     k_deal_batched<<<std::max(1, dgrid), 128, 0, b->stream>>>(b->d_tables, b->d_phases + p, T, b->d_deals);
     BCK(cudaGetLastError());
     BCK(rec(b->ev_ph[2 * p]));
-    kern<<<grid, t.block, smem, b->stream>>>(b->d_tables, b->d_phases + p, b->d_deals, b->d_work + p, t.grab);
+    kern<<<grid, t.block, smem, b->stream>>>(b->params[p], b->d_deals, b->d_work + p, t.grab, t.warp_sync);
     BCK(cudaGetLastError());
     BCK(rec(b->ev_ph[2 * p + 1]));
     k_apply_batched<<<dim3(148 * 2, P.n), 256, 0, b->stream>>>(b->d_tables, b->d_phases + p);
@@ -1434,6 +1438,14 @@ int mccfr_batch_create(mccfr_handle* const* tables, int n, const int* traversals
     P.off[P.n] = off;
     b->max_items = std::max(b->max_items, off);
   }
+  b->params.resize(b->max_players);
+  for (int p = 0; p < b->max_players; ++p) {
+    PhaseParams& Q = b->params[p];
+    std::memset(&Q, 0, sizeof(Q));
+    Q.n = b->phases[p].n;
+    for (int j = 0; j <= Q.n; ++j) Q.off[j] = b->phases[p].off[j];
+    for (int j = 0; j < Q.n; ++j) Q.T[j] = descs[b->phases[p].table[j]];
+  }
   if (cudaMalloc(&b->d_tables, n * sizeof(TableDesc)) != cudaSuccess ||
       cudaMalloc(&b->d_phases, b->max_players * sizeof(PhaseDesc)) != cudaSuccess ||
       cudaMalloc(&b->d_work, b->max_players * sizeof(unsigned long long)) != cudaSuccess ||
@@ -1514,15 +1526,28 @@ int mccfr_batch_autotune(mccfr_batch* b, int max_candidates, mccfr_batch_tuning*
   if (!b) return MCCFR_ERR_INVALID_ARG;
   BCK(cudaSetDevice(b->device));
   std::vector<mccfr_batch_tuning> cands;
+  // most informative dimensions first: a prefix of the list is a useful sweep
   for (int blk : {128, 64, 256})
-    for (int grab : {2, 1, 4, 8})
+    for (int grab : {1, 2, 4, 8})
       for (int k : {0, 2, 4})
-        for (int w : {1, 2}) cands.push_back(mccfr_batch_tuning{blk, grab, k, w, {0, 0, 0, 0}});
+        for (int ws : {1, 0})
+          for (int w : {1, 2}) cands.push_back(mccfr_batch_tuning{blk, grab, k, w, ws, {0, 0, 0}});
   if (max_candidates > 0 && (int)cands.size() > max_candidates) cands.resize(max_candidates);
-  double best_ms = 1e300;
+  // Candidates run on successive real iterations, whose trees shrink as the
+  // strategy sharpens, so they are ranked by traversal-kernel time per node visit.
+  auto visits_now = [&]() {
+    unsigned long long v = 0;
+    for (mccfr_handle* h : b->tables) {
+      Counters c;
+      if (cudaMemcpy(&c, h->d_counters, sizeof(c), cudaMemcpyDeviceToHost) == cudaSuccess) v += c.visits;
+    }
+    return v;
+  };
+  double best_cost = 1e300;
   mccfr_batch_tuning best_t = b->tuning;
   for (const mccfr_batch_tuning& t : cands) {
     b->tuning = t;
+    const unsigned long long v0 = visits_now();
     int rc = batch_set_scheds(b);
     if (rc) return rc;
     rc = batch_enqueue_iteration(b, false);
@@ -1540,8 +1565,9 @@ int mccfr_batch_autotune(mccfr_batch* b, int max_candidates, mccfr_batch_tuning*
     b->total_ms += it_ms;
     rc = batch_after(b, 1);
     if (rc) return rc;
-    if (trav < best_ms) {
-      best_ms = trav;
+    const double cost = trav / (double)std::max(1ull, visits_now() - v0);
+    if (cost < best_cost) {
+      best_cost = cost;
       best_t = t;
     }
   }

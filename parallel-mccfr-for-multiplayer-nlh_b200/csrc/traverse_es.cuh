@@ -303,6 +303,11 @@ inline void launch_traverse_es(const GameParams& G, const TableView& tv, const D
                                int batch, float rscale, Counters* counters, cudaStream_t stream) {
   constexpr int B = 128;
   const int grid = (batch + B - 1) / B;
+  static bool carveout_set = false;  // the walk keeps no shared memory: all of it to L1
+  if (!carveout_set) {
+    cudaFuncSetAttribute(k_traverse_es<B, 0, 1>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    carveout_set = true;
+  }
   k_traverse_es<B, 0, 1><<<grid, B, 0, stream>>>(G, tv, deals, sched, batch, rscale, counters);
 }
 

@@ -68,11 +68,11 @@ class Stats(Structure):
 
 class BatchTuning(Structure):
     _fields_ = [("block", c_int32), ("grab", c_int32), ("smem_frames", c_int32), ("probe_width", c_int32),
-                ("reserved", c_int32 * 4)]
+                ("warp_sync", c_int32), ("reserved", c_int32 * 3)]
 
     def as_dict(self) -> dict:
         return {"block": self.block, "grab": self.grab, "smem_frames": self.smem_frames,
-                "probe_width": self.probe_width}
+                "probe_width": self.probe_width, "warp_sync": self.warp_sync}
 
 
 class BatchStats(Structure):

@@ -208,11 +208,12 @@ class Batch:
 
     @staticmethod
     def candidates(max_candidates: int = 0) -> list:
-        c = [(b, g, k, w) for b in (128, 64, 256) for g in (2, 1, 4, 8) for k in (0, 2, 4) for w in (1, 2)]
+        c = [dict(block=b, grab=g, smem_frames=k, probe_width=w, warp_sync=s)
+             for b in (128, 64, 256) for g in (1, 2, 4, 8) for k in (0, 2, 4) for s in (1, 0) for w in (1, 2)]
         return c[:max_candidates] if max_candidates > 0 else c
 
-    def set_tuning(self, block=128, grab=2, smem_frames=0, probe_width=1) -> None:
-        t = L.BatchTuning(block, grab, smem_frames, probe_width)
+    def set_tuning(self, block=128, grab=2, smem_frames=0, probe_width=1, warp_sync=1) -> None:
+        t = L.BatchTuning(block, grab, smem_frames, probe_width, warp_sync)
         L.check(self._lib.mccfr_batch_set_tuning(self._b, byref(t)))
 
     def tuning(self) -> dict:
