@@ -278,6 +278,37 @@ int mccfr_batch_train(mccfr_batch* b, long long iters, int flags);
 int mccfr_batch_autotune(mccfr_batch* b, int max_candidates, mccfr_batch_tuning* best);
 int mccfr_batch_get_stats(mccfr_batch* b, mccfr_batch_stats* out);
 
+/* ---- subgame re-solve and continuous batching -----------------------------
+   No reference counterpart.  A subgame starts on the turn or the
+   river with a known board, a dead pot shared equally by the players, equal
+   stacks (cfg->starting_stack), and one 1326-combo range per player (combo of
+   cards lo < hi is index hi*(hi-1)/2 + lo; combos that use a board card get
+   weight 0).  Hole combos are drawn from the ranges with card removal; info
+   sets are keyed by the exact combo (and the river card on the river).  The
+   subgame uses external sampling and 64-bit keys. */
+typedef struct mccfr_subgame {
+  int32_t street;         /* 2 = turn (4 board cards), 3 = river (5) */
+  int32_t pot;            /* chips in the pot; must be a multiple of num_players */
+  uint8_t board[5];
+  uint8_t pad[3];
+  const float* ranges;    /* [num_players][1326] non-negative weights */
+} mccfr_subgame;
+int mccfr_create_subgame(const mccfr_config* cfg, const mccfr_subgame* sg, mccfr_handle** out);
+/* Makes h use src's device rank table instead of uploading its own (src must
+   outlive h).  Valid for subgames and for tables without rank-CDF buckets or
+   with the same bucket counts as src. */
+int mccfr_share_hand_table(mccfr_handle* h, mccfr_handle* src);
+/* One player-update of each listed table, all in one persistent traversal
+   launch: the serving step of continuous batching.  Each table advances its
+   own (iteration, player) and its iteration count after its last player.
+   traversals[i] = traversals of table i's update; tuning may be NULL. */
+int mccfr_batch_round(mccfr_handle* const* tables, int n, const int* traversals,
+                      const mccfr_batch_tuning* tuning);
+/* The (iteration, player) the table's next update will run, and the number of
+   completed iterations. */
+int mccfr_get_progress(mccfr_handle* h, long long* next_iteration, int* next_player,
+                       long long* iterations_done);
+
 /* ---- evaluation without device allocation --------------------------------
    No counterpart in the reference.  For callers that cannot allocate device
    memory (code inside a framework that owns every device allocation, or a

@@ -50,6 +50,9 @@ def lib() -> ctypes.CDLL:
         o.orc_valid_mask.argtypes = [c_void_p, c_int, c_int, c_int, c_int, c_int, c_int]
         o.orc_chips.argtypes = [c_void_p, c_int, c_int, c_int, c_int, c_int, c_int]
         o.orc_regret_frac_bits.argtypes = [c_void_p, c_longlong]
+        o.orc_create_subgame.restype = c_void_p
+        o.orc_create_subgame.argtypes = [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p]
+        o.orc_range_cdf.argtypes = [c_void_p, c_void_p, c_int, c_void_p]
         o.brute_rank.argtypes = [c_void_p, c_int]
         o.brute_rank_batch.argtypes = [c_void_p, c_int, c_void_p, c_size_t, c_int]
         _orc = o
@@ -59,10 +62,22 @@ def lib() -> ctypes.CDLL:
 class Oracle:
     """CPU restatement of one trainer (same config struct as the product)."""
 
-    def __init__(self, config, hand_table: np.ndarray):
+    def __init__(self, config, hand_table: np.ndarray, subgame: dict | None = None):
         self._t = np.ascontiguousarray(hand_table, dtype=np.int32)  # kept alive (borrowed by C)
         self._cfg = config
-        self._h = lib().orc_create(ctypes.byref(config), _p(self._t))
+        if subgame is None:
+            self._h = lib().orc_create(ctypes.byref(config), _p(self._t))
+            return
+        board = np.zeros(5, dtype=np.uint8)
+        nb = 4 if subgame["street"] == 2 else 5
+        board[:nb] = subgame["board"][:nb]
+        ranges = np.ascontiguousarray(subgame["ranges"], dtype=np.float32).reshape(config.num_players, 1326)
+        cdf = np.zeros((config.num_players, 1326), dtype=np.uint32)
+        for p in range(config.num_players):
+            assert lib().orc_range_cdf(_p(ranges[p]), _p(board), nb, _p(cdf[p])) == 1
+        self._cdf = cdf
+        self._h = lib().orc_create_subgame(ctypes.byref(config), _p(self._t), subgame["street"], subgame["pot"],
+                                           _p(board), _p(cdf))
 
     def close(self):
         if self._h:

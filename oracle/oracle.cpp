@@ -368,6 +368,8 @@ static int passive_fallback(const Rules& R, uint8_t vm) {  // cfr_gpu.cu:498-508
 // ---------------------------------------------------------------------------
 struct Game {
   int N;
+  uint32_t combo[6];
+  int river_card;
   uint8_t hole[12];
   uint8_t board[5];
   uint8_t hole_b[6];
@@ -429,7 +431,15 @@ struct Counters {
   int64_t V = 0, U = 0, T = 0, E = 0, X = 0;
 };
 
+struct Subgame {
+  int street = 0;  // 0 = full game
+  int pot = 0;
+  uint8_t board[5] = {0, 0, 0, 0, 0};
+  std::vector<uint32_t> cdf;  // [N][1326]
+};
+
 struct Oracle {
+  Subgame sg;
   Rules R;
   const int32_t* T = nullptr;
   uint8_t pre_lut[52 * 52];
@@ -477,8 +487,12 @@ static inline const Row* find_row(const Oracle& O, uint64_t key) {
 }
 
 static uint64_t info_key(const Oracle& O, const Game& g, int player) {
-  const int hb = g.hole_b[player];
-  const int bb = g.board_b[player][g.street];
+  int hb = g.hole_b[player];
+  int bb = g.board_b[player][g.street];
+  if (O.sg.street) {  // subgame: exact combo, and the river card on the river
+    hb = (int)g.combo[player];
+    bb = (g.street == 3 && O.sg.street == 2) ? g.river_card + 1 : 0;
+  }
   if (O.R.c.key_mode == MCCFR_KEY_FNV26)
     return (uint64_t)fnv_slot(player, hb, bb, g.street, g.abits) + 1;
   uint64_t k = g.path ^ ((uint64_t)player << 56) ^ ((uint64_t)hb << 44) ^
@@ -732,8 +746,131 @@ static float traverse(Ctx& C, Game& g, int depth) {  // cfr_gpu.cu:644-860
   return traverse(C, ch, depth + 1);
 }
 
+static int combo_of(int a, int b) {
+  const int lo = std::min(a, b), hi = std::max(a, b);
+  return hi * (hi - 1) / 2 + lo;
+}
+static void cards_of(int idx, int& lo, int& hi) {
+  int h = 1;
+  while ((h + 1) * h / 2 <= idx) ++h;
+  hi = h;
+  lo = idx - h * (h - 1) / 2;
+}
+static int sample_combo(const uint32_t* cdf, uint32_t w) {
+  int lo = 0, hi = 1325;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (w < cdf[mid]) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo;
+}
+
+// Subgame traversal: combos from the ranges with card removal (joint redraws,
+// then a player-by-player fallback), the river card uniform among unused cards.
+static void run_subgame_traversal(Ctx& C) {
+  const Oracle& O = *C.O;
+  const Rules& R = O.R;
+  const int N = std::min(6, std::max(2, R.c.num_players));
+  const uint32_t k0 = (uint32_t)R.c.seed, k1 = (uint32_t)(R.c.seed >> 32);
+  const int nb = O.sg.street == 2 ? 4 : 5;
+  uint64_t board_mask = 0;
+  for (int i = 0; i < nb; ++i) board_mask |= 1ull << O.sg.board[i];
+  int combo[6] = {0, 0, 0, 0, 0, 0};
+  uint64_t used = board_mask;
+  bool ok = false;
+  for (int a = 0; a < 16 && !ok; ++a) {
+    const U4 w0 = philox(U4{C.t, C.launch, 0x100u + (uint32_t)a, 0u}, k0, k1);
+    const U4 w1 = philox(U4{C.t, C.launch, 0x100u + (uint32_t)a, 1u}, k0, k1);
+    const uint32_t words[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+    used = board_mask;
+    ok = true;
+    for (int p = 0; p < N && ok; ++p) {
+      combo[p] = sample_combo(O.sg.cdf.data() + 1326 * p, words[p] >> 1);
+      int lo, hi;
+      cards_of(combo[p], lo, hi);
+      const uint64_t m = (1ull << lo) | (1ull << hi);
+      if (used & m) ok = false;
+      used |= m;
+    }
+  }
+  if (!ok) {
+    const U4 w0 = philox(U4{C.t, C.launch, 0x100u, 0u}, k0, k1);
+    const U4 w1 = philox(U4{C.t, C.launch, 0x100u, 1u}, k0, k1);
+    const uint32_t words[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+    used = board_mask;
+    for (int p = 0; p < N; ++p) {
+      const uint32_t* cdf = O.sg.cdf.data() + 1326 * p;
+      const int start = sample_combo(cdf, words[p] >> 1);
+      int pick = -1;
+      for (int k = 0; k < 1326 && pick < 0; ++k) {
+        const int c = (start + k) % 1326;
+        const uint32_t prev = c ? cdf[c - 1] : 0u;
+        if (cdf[c] == prev) continue;
+        int lo, hi;
+        cards_of(c, lo, hi);
+        if (!(used & ((1ull << lo) | (1ull << hi)))) pick = c;
+      }
+      if (pick < 0) pick = start;
+      combo[p] = pick;
+      int lo, hi;
+      cards_of(pick, lo, hi);
+      used |= (1ull << lo) | (1ull << hi);
+    }
+  }
+  Game g;
+  std::memset(&g, 0, sizeof(g));
+  g.N = N;
+  for (int i = 0; i < nb; ++i) g.board[i] = O.sg.board[i];
+  g.river_card = -1;
+  if (nb == 4) {
+    const U4 w = philox(U4{C.t, C.launch, 0x200u, 0u}, k0, k1);
+    const int free_cards = 52 - __builtin_popcountll(used);
+    int k = (int)(((uint64_t)w.x * (uint64_t)free_cards) >> 32);
+    for (int c = 0; c < 52; ++c) {
+      if ((used >> c) & 1) continue;
+      if (k-- == 0) {
+        g.river_card = c;
+        break;
+      }
+    }
+    g.board[4] = (uint8_t)g.river_card;
+  }
+  for (int p = 0; p < N; ++p) {
+    int lo, hi;
+    cards_of(combo[p], lo, hi);
+    g.hole[2 * p] = (uint8_t)lo;
+    g.hole[2 * p + 1] = (uint8_t)hi;
+    g.combo[p] = (uint32_t)combo[p];
+    int cards[7] = {lo, hi, g.board[0], g.board[1], g.board[2], g.board[3], g.board[4]};
+    g.river_rank[p] = decode16((uint16_t)chain(O.T, cards, 7));
+  }
+  C.cnt->E += N;
+  g.dealer = N - 1;
+  for (int i = 0; i < N; ++i) {
+    g.stacks[i] = R.c.starting_stack;
+    g.bets[i] = 0;
+    g.inv[i] = O.sg.pot / N;
+  }
+  g.pot = O.sg.pot;
+  g.cb = 0;
+  g.lfr = R.c.big_blind;
+  g.abits = 0;
+  g.path = kPathSeed;
+  g.street = O.sg.street;
+  g.raises = 0;
+  g.n_to_act = 0;
+  for (int i = 1; i <= N; ++i) g.to_act[g.n_to_act++] = (g.dealer + i) % N;
+  C.cnt->T++;
+  traverse(C, g, 0);
+}
+
 // One traversal: deal, buckets, blinds, walk (cfr_gpu.cu:916-987).
 static void run_traversal(Ctx& C) {
+  if (C.O->sg.street) {
+    run_subgame_traversal(C);
+    return;
+  }
   const Oracle& O = *C.O;
   const Rules& R = O.R;
   const int N = std::min(6, std::max(2, R.c.num_players));
@@ -936,6 +1073,47 @@ void* orc_create(const mccfr_config* cfg, const int32_t* hand_table) {
 }
 
 void orc_destroy(void* h) { delete (Oracle*)h; }
+
+// Subgame oracle; cdf is the [N][1326] range CDF on the 2^31 scale.
+void* orc_create_subgame(const mccfr_config* cfg, const int32_t* hand_table, int street, int pot,
+                         const uint8_t* board, const uint32_t* cdf) {
+  Oracle* O = (Oracle*)orc_create(cfg, hand_table);
+  O->sg.street = street;
+  O->sg.pot = pot;
+  for (int i = 0; i < 5; ++i) O->sg.board[i] = board[i];
+  O->sg.cdf.assign(cdf, cdf + 1326 * cfg->num_players);
+  return O;
+}
+
+// Range CDF on the 2^31 scale (combos using a board card weigh 0; the last
+// combo of positive weight ends at 2^31).  Returns 0 when the range is empty.
+int orc_range_cdf(const float* w, const uint8_t* board, int nb, uint32_t* out) {
+  uint64_t mask = 0;
+  for (int i = 0; i < nb; ++i) mask |= 1ull << board[i];
+  double total = 0.0;
+  for (int c = 0; c < 1326; ++c) {
+    int lo, hi;
+    cards_of(c, lo, hi);
+    const bool blocked = ((mask >> lo) & 1) || ((mask >> hi) & 1);
+    total += (!blocked && w[c] > 0.0f) ? (double)w[c] : 0.0;
+  }
+  if (!(total > 0.0)) return 0;
+  double cum = 0.0;
+  int last = -1;
+  for (int c = 0; c < 1326; ++c) {
+    int lo, hi;
+    cards_of(c, lo, hi);
+    const bool blocked = ((mask >> lo) & 1) || ((mask >> hi) & 1);
+    const double x = (!blocked && w[c] > 0.0f) ? (double)w[c] : 0.0;
+    cum += x;
+    if (x > 0.0) last = c;
+    double v = std::floor(cum / total * 2147483648.0);
+    if (v > 2147483648.0) v = 2147483648.0;
+    out[c] = (uint32_t)v;
+  }
+  for (int c = last; c < 1326; ++c) out[c] = 2147483648u;
+  return 1;
+}
 
 void orc_set_float_mode(void* h, int on) { ((Oracle*)h)->float_mode = on != 0; }
 

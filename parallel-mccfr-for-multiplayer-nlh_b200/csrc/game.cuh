@@ -21,6 +21,11 @@ struct GameParams {
   int post_b[3];
   uint32_t seed_lo, seed_hi;
   int key_bits;
+  // subgame re-solve (sub_street 0 = the full game from the blinds)
+  int sub_street;               // 2: starts on the turn, 3: on the river
+  int sub_pot;                  // chips already in the pot, split equally
+  uint8_t sub_board[5];         // known board cards (4 or 5)
+  const uint32_t* range_cdf;    // [N][1326] cumulative range weights, 2^31 scale
   // action slots
   int8_t kind[kSlots];
   int16_t num[kSlots], den[kSlots];
@@ -204,6 +209,18 @@ __device__ __forceinline__ void node_strategy(const float* reg, uint32_t vm, flo
 #pragma unroll
     for (int a = 0; a < kSlots; ++a) strat[a] = ((vm >> a) & 1) ? uni : 0.0f;
   }
+}
+
+// Hole-card combo index of two distinct cards: hi*(hi-1)/2 + lo, 0..1325.
+__device__ __forceinline__ int combo_index(int a, int b) {
+  const int lo = min(a, b), hi = max(a, b);
+  return hi * (hi - 1) / 2 + lo;
+}
+__device__ __forceinline__ void combo_cards(int idx, int& lo, int& hi) {
+  int h = 1;
+  while ((h + 1) * h / 2 <= idx) ++h;
+  hi = h;
+  lo = idx - h * (h - 1) / 2;
 }
 
 // Reference info-set slot (cfr_gpu.cu:165-179).

@@ -20,6 +20,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -279,6 +280,9 @@ struct mccfr_handle {
   Sched* d_sched = nullptr;
   DealRec* d_deals = nullptr;  // one record per traversal of an update
   int deals_cap = 0;
+  uint32_t* d_ranges = nullptr;  // subgame range CDFs [N][1326]
+  bool shared_hr = false;        // d_hr borrowed from another handle
+  int round_player = 0;          // next player of round-by-round training
   Sched* h_sched = nullptr;  // pinned
   Counters* d_counters = nullptr;
   // graph of one iteration
@@ -606,7 +610,8 @@ void release(mccfr_handle* h) {
     if (e) cudaEventDestroy(e);
   for (auto& e : h->gev)
     if (e) cudaEventDestroy(e);
-  cudaFree(h->d_hr);
+  if (!h->shared_hr) cudaFree(h->d_hr);
+  cudaFree(h->d_ranges);
   cudaFree(h->d_pre);
   cudaFree(h->d_cdf);
   cudaFree(h->d_block);
@@ -1595,6 +1600,229 @@ int mccfr_batch_get_stats(mccfr_batch* b, mccfr_batch_stats* out) {
   out->traverse_ms = b->traverse_ms;
   out->total_ms = b->total_ms;
   return MCCFR_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Subgames and continuous batching.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct RoundCtx {
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  TableDesc* d_tables = nullptr;
+  PhaseDesc* d_phase = nullptr;
+  DealRec* d_deals = nullptr;
+  unsigned long long* d_work = nullptr;
+  size_t deals_cap = 0;
+  PhaseParams params;
+};
+
+RoundCtx g_round[64];
+std::mutex g_round_mu;
+
+// Range CDF on the 2^31 scale: combos that use a board card weigh 0; the last
+// combo of positive weight ends at exactly 2^31.
+bool build_range_cdf(const float* w, uint64_t board_mask, uint32_t* out) {
+  double total = 0.0;
+  for (int c = 0; c < 1326; ++c) {
+    int hi = 1;
+    while ((hi + 1) * hi / 2 <= c) ++hi;
+    const int lo = c - hi * (hi - 1) / 2;
+    const bool blocked = ((board_mask >> lo) & 1) || ((board_mask >> hi) & 1);
+    const double x = (!blocked && w[c] > 0.0f) ? (double)w[c] : 0.0;
+    total += x;
+  }
+  if (!(total > 0.0)) return false;
+  double cum = 0.0;
+  int last = -1;
+  for (int c = 0; c < 1326; ++c) {
+    int hi = 1;
+    while ((hi + 1) * hi / 2 <= c) ++hi;
+    const int lo = c - hi * (hi - 1) / 2;
+    const bool blocked = ((board_mask >> lo) & 1) || ((board_mask >> hi) & 1);
+    const double x = (!blocked && w[c] > 0.0f) ? (double)w[c] : 0.0;
+    cum += x;
+    if (x > 0.0) last = c;
+    double v = std::floor(cum / total * 2147483648.0);
+    if (v > 2147483648.0) v = 2147483648.0;
+    out[c] = (uint32_t)v;
+  }
+  for (int c = last; c < 1326; ++c) out[c] = 2147483648u;
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mccfr_create_subgame(const mccfr_config* cfg, const mccfr_subgame* sg, mccfr_handle** out) {
+  if (!cfg || !sg || !out || !sg->ranges) return MCCFR_ERR_INVALID_ARG;
+  if (cfg->sampling != MCCFR_SAMPLING_EXTERNAL || cfg->key_mode != MCCFR_KEY_ID64) {
+    fprintf(stderr, "mccfr_create_subgame: subgames use external sampling and ID64 keys\n");
+    return MCCFR_ERR_INVALID_ARG;
+  }
+  if (sg->street != 2 && sg->street != 3) return MCCFR_ERR_INVALID_ARG;
+  const int nb = sg->street == 2 ? 4 : 5;
+  uint64_t mask = 0;
+  for (int i = 0; i < nb; ++i) {
+    if (sg->board[i] > 51 || ((mask >> sg->board[i]) & 1)) return MCCFR_ERR_INVALID_ARG;
+    mask |= 1ull << sg->board[i];
+  }
+  if (sg->pot < 0 || sg->pot % cfg->num_players != 0 || sg->pot / cfg->num_players > 65535)
+    return MCCFR_ERR_INVALID_ARG;
+  std::vector<uint32_t> cdf((size_t)cfg->num_players * 1326);
+  for (int p = 0; p < cfg->num_players; ++p)
+    if (!build_range_cdf(sg->ranges + 1326 * p, mask, cdf.data() + 1326 * p)) {
+      fprintf(stderr, "mccfr_create_subgame: player %d's range has no weight off the board\n", p);
+      return MCCFR_ERR_INVALID_ARG;
+    }
+  const int rc = mccfr_create(cfg, out);
+  if (rc) return rc;
+  mccfr_handle* h = *out;
+  if (cudaMalloc(&h->d_ranges, cdf.size() * 4) != cudaSuccess ||
+      cudaMemcpy(h->d_ranges, cdf.data(), cdf.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+    mccfr_destroy(h);
+    *out = nullptr;
+    return MCCFR_ERR_OOM;
+  }
+  h->gp.sub_street = sg->street;
+  h->gp.sub_pot = sg->pot;
+  for (int i = 0; i < 5; ++i) h->gp.sub_board[i] = (i < nb) ? sg->board[i] : 0;
+  h->gp.range_cdf = h->d_ranges;
+  return MCCFR_OK;
+}
+
+int mccfr_share_hand_table(mccfr_handle* h, mccfr_handle* src) {
+  if (!h || !src || !src->has_table || h->device != src->device) return MCCFR_ERR_INVALID_ARG;
+  if (h->cfg.postflop_mode == MCCFR_POSTFLOP_RANK_CDF && !h->gp.sub_street) {
+    if (src->cfg.postflop_mode != MCCFR_POSTFLOP_RANK_CDF ||
+        std::memcmp(src->cfg.postflop_buckets, h->cfg.postflop_buckets, sizeof(h->cfg.postflop_buckets)))
+      return fail(h, MCCFR_ERR_INVALID_ARG, "rank-CDF buckets differ from the source table's");
+    CK(cudaMemcpy(h->d_cdf, src->d_cdf, 3 * 7463, cudaMemcpyDeviceToDevice));
+  }
+  if (h->d_hr && !h->shared_hr) cudaFree(h->d_hr);
+  h->d_hr = src->d_hr;
+  h->shared_hr = true;
+  h->has_table = true;
+  if (h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+    h->graph_batch = -1;
+  }
+  return MCCFR_OK;
+}
+
+int mccfr_get_progress(mccfr_handle* h, long long* next_iteration, int* next_player, long long* done) {
+  if (!h) return MCCFR_ERR_INVALID_ARG;
+  if (next_iteration) *next_iteration = h->iterations_done + 1;
+  if (next_player) *next_player = h->round_player;
+  if (done) *done = h->iterations_done;
+  return MCCFR_OK;
+}
+
+int mccfr_batch_round(mccfr_handle* const* tables, int n, const int* traversals, const mccfr_batch_tuning* tuning) {
+  if (!tables || !traversals || n < 1 || n > kMaxBatchTables) return MCCFR_ERR_INVALID_ARG;
+  mccfr_batch_tuning t{128, 1, 0, 1, 1, {0, 0, 0}};
+  if (tuning) {
+    if (!valid_tuning(*tuning)) return MCCFR_ERR_INVALID_ARG;
+    t = *tuning;
+  }
+  const int dev = tables[0]->device;
+  for (int i = 0; i < n; ++i) {
+    mccfr_handle* h = tables[i];
+    if (!h || !h->has_table || h->device != dev || traversals[i] < 1 || h->cfg.sampling != MCCFR_SAMPLING_EXTERNAL)
+      return MCCFR_ERR_INVALID_ARG;
+  }
+  if (dev < 0 || dev >= 64) return MCCFR_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lock(g_round_mu);
+  RoundCtx& R = g_round[dev];
+  mccfr_batch* b = nullptr;  // for BCK error reporting
+  BCK(cudaSetDevice(dev));
+  if (!R.stream) {
+    BCK(cudaStreamCreateWithFlags(&R.stream, cudaStreamNonBlocking));
+    BCK(cudaMalloc(&R.d_tables, kMaxBatchTables * sizeof(TableDesc)));
+    BCK(cudaMalloc(&R.d_phase, sizeof(PhaseDesc)));
+    BCK(cudaMalloc(&R.d_work, sizeof(unsigned long long)));
+    R.device = dev;
+  }
+  unsigned long long total = 0;
+  for (int i = 0; i < n; ++i) total += (unsigned long long)traversals[i];
+  if (total > R.deals_cap) {
+    cudaFree(R.d_deals);
+    R.d_deals = nullptr;
+    BCK(cudaMalloc(&R.d_deals, total * sizeof(DealRec)));
+    R.deals_cap = total;
+  }
+  std::vector<TableDesc> descs(n);
+  PhaseDesc P;
+  std::memset(&P, 0, sizeof(P));
+  PhaseParams& Q = R.params;
+  std::memset(&Q, 0, sizeof(Q));
+  unsigned long long off = 0;
+  for (int i = 0; i < n; ++i) {
+    mccfr_handle* h = tables[i];
+    h->h_sched->iteration = h->iterations_done + 1;
+    h->h_sched->player = h->round_player;
+    h->h_sched->pad = 0;
+    BCK(cudaMemcpyAsync(h->d_sched, h->h_sched, sizeof(Sched), cudaMemcpyHostToDevice, R.stream));
+    TableDesc& d = descs[i];
+    std::memset(&d, 0, sizeof(d));
+    d.G = h->gp;
+    d.tv = h->tv;
+    d.pre = h->d_pre;
+    d.cdf = h->d_cdf;
+    d.sched = h->d_sched;
+    d.counters = h->d_counters;
+    const int rb = regret_frac_bits(h->cfg, traversals[i]);
+    d.rscale = std::ldexp(1.0f, rb);
+    d.rinv = std::ldexp(1.0, -rb);
+    d.batch = traversals[i];
+    P.table[i] = i;
+    P.off[i] = off;
+    Q.off[i] = off;
+    Q.T[i] = d;
+    off += (unsigned long long)traversals[i];
+  }
+  P.n = n;
+  P.off[n] = off;
+  Q.n = n;
+  Q.off[n] = off;
+  BCK(cudaMemcpyAsync(R.d_tables, descs.data(), n * sizeof(TableDesc), cudaMemcpyHostToDevice, R.stream));
+  BCK(cudaMemcpyAsync(R.d_phase, &P, sizeof(P), cudaMemcpyHostToDevice, R.stream));
+  BCK(cudaMemsetAsync(R.d_work, 0, sizeof(unsigned long long), R.stream));
+  const int dgrid = (int)std::min<unsigned long long>((off + 127) / 128, 148ull * 64);
+  k_deal_batched<<<std::max(1, dgrid), 128, 0, R.stream>>>(R.d_tables, R.d_phase, tables[0]->d_hr, R.d_deals);
+  BCK(cudaGetLastError());
+  BatchedKernel kern = pick_kernel(t);
+  const size_t smem = batched_smem(t);
+  BCK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, t.block, smem));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const unsigned long long need_blocks = (off + t.block - 1) / t.block;
+  const int grid = (int)std::max<unsigned long long>(1, std::min<unsigned long long>(need_blocks, (unsigned long long)std::max(1, per_sm) * sms));
+  kern<<<grid, t.block, smem, R.stream>>>(Q, R.d_deals, R.d_work, t.grab, t.warp_sync);
+  BCK(cudaGetLastError());
+  k_apply_batched<<<dim3(std::max(1, std::min(148 * 2, (int)((off * 8 + 255) / 256) + 1)), n), 256, 0, R.stream>>>(
+      R.d_tables, R.d_phase);
+  BCK(cudaGetLastError());
+  BCK(cudaStreamSynchronize(R.stream));
+  int worst = MCCFR_OK;
+  for (int i = 0; i < n; ++i) {
+    mccfr_handle* h = tables[i];
+    h->launches++;
+    if (++h->round_player >= h->cfg.num_players) {
+      h->round_player = 0;
+      h->iterations_done++;
+    }
+    const int rc = check_device_error(h);
+    if (rc && !worst) worst = rc;
+  }
+  return worst;
 }
 
 }  // extern "C"

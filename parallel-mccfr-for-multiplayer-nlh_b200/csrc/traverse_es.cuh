@@ -109,7 +109,28 @@ __device__ __forceinline__ void es_walk(const GameParams& G, const TableView& tv
     rank[p] = D.rank[p];
   }
   EsState cur;
-  {
+  if (G.sub_street) {
+    // subgame: the dead pot split equally, everyone with the same stack, first
+    // to act after the dealer (the last seat)
+    for (int p = 0; p < kMaxPlayers; ++p) {
+      cur.stack[p] = (uint16_t)G.stack;
+      cur.bet[p] = 0;
+      cur.inv[p] = (uint16_t)((p < N) ? G.sub_pot / N : 0);
+    }
+    cur.pot = G.sub_pot;
+    cur.cb = 0;
+    cur.lfr = G.bb;
+    cur.folded = 0;
+    cur.allin = 0;
+    cur.street = (uint8_t)G.sub_street;
+    cur.raises = 0;
+    cur.abits = 0;
+    cur.path = kPathSeed;
+    cur.depth = 0;
+    cur.q = 0;
+    cur.nq = 0;
+    for (int i = 1; i <= N; ++i) cur.q |= (uint32_t)((dealer + i) % N) << (4 * cur.nq++);
+  } else {
     for (int p = 0; p < kMaxPlayers; ++p) {
       cur.stack[p] = (uint16_t)G.stack;
       cur.bet[p] = 0;
@@ -193,8 +214,14 @@ __device__ __forceinline__ void es_walk(const GameParams& G, const TableView& tv
       const int to_call = cur.cb - (int)cur.bet[player];
       const uint32_t vm = valid_mask(G, cur.pot, cur.stack[player], to_call, cur.cb, cur.lfr, cur.raises);
       const uint32_t cw = ctx[player];
-      const uint32_t hb = cw & 0xFF;
-      const uint32_t bkt = cur.street ? ((cw >> (8 * cur.street)) & 0xFF) : 0u;
+      uint32_t hb, bkt;
+      if (G.sub_street) {  // exact combo; the river card once it is dealt
+        hb = cw & 0xFFFF;
+        bkt = (cur.street == 3 && G.sub_street == 2) ? (cw >> 16) : 0u;
+      } else {
+        hb = cw & 0xFF;
+        bkt = cur.street ? ((cw >> (8 * cur.street)) & 0xFF) : 0u;
+      }
       const unsigned long long key = info_key(G, player, hb, bkt, cur.street, cur.abits, cur.path);
       const long long slot = table_insert<W>(tv, key);
       float reg[kSlots];

@@ -76,12 +76,119 @@ __device__ __forceinline__ uint32_t update_id(const Sched* s, int N) {
   return (uint32_t)((s->iteration - 1) * N + s->player);
 }
 
+// First combo whose cumulative weight exceeds w (w < 2^31), by bisection.
+__device__ __forceinline__ int sample_combo(const uint32_t* __restrict__ cdf, uint32_t w) {
+  int lo = 0, hi = 1325;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (w < __ldg(cdf + mid)) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo;
+}
+
+// Subgame deal: every player's hole combo from its range, all combos drawn
+// together and redrawn (up to 16 times) until no two share a card; after that,
+// player by player, the drawn combo or the next one of positive weight that
+// fits.  On the turn the river card is then uniform among the unused cards.
+// ctx[p] = combo | (river card + 1) << 16 (the river card enters the river keys).
+__device__ __forceinline__ void deal_subgame(const GameParams& G, const int32_t* __restrict__ T, uint32_t t,
+                                             uint32_t uid, DealRec* __restrict__ out) {
+  const int N = G.N;
+  const int nb = G.sub_street == 2 ? 4 : 5;
+  uint64_t used_board = 0;
+  for (int i = 0; i < nb; ++i) used_board |= 1ull << G.sub_board[i];
+  int combo[kMaxPlayers];
+  uint64_t used = used_board;
+  bool ok = false;
+  for (int a = 0; a < 16 && !ok; ++a) {
+    const U4 w0 = philox(U4{t, uid, 0x100u + (uint32_t)a, 0u}, G.seed_lo, G.seed_hi);
+    const U4 w1 = philox(U4{t, uid, 0x100u + (uint32_t)a, 1u}, G.seed_lo, G.seed_hi);
+    const uint32_t words[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+    used = used_board;
+    ok = true;
+    for (int p = 0; p < N && ok; ++p) {
+      combo[p] = sample_combo(G.range_cdf + 1326 * p, words[p] >> 1);
+      int lo, hi;
+      combo_cards(combo[p], lo, hi);
+      const uint64_t m = (1ull << lo) | (1ull << hi);
+      if (used & m) ok = false;
+      used |= m;
+    }
+  }
+  if (!ok) {
+    const U4 w0 = philox(U4{t, uid, 0x100u, 0u}, G.seed_lo, G.seed_hi);
+    const U4 w1 = philox(U4{t, uid, 0x100u, 1u}, G.seed_lo, G.seed_hi);
+    const uint32_t words[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+    used = used_board;
+    for (int p = 0; p < N; ++p) {
+      const uint32_t* cdf = G.range_cdf + 1326 * p;
+      const int start = sample_combo(cdf, words[p] >> 1);
+      int pick = -1;
+      for (int k = 0; k < 1326 && pick < 0; ++k) {
+        const int c = (start + k) % 1326;
+        const uint32_t prev = c ? __ldg(cdf + c - 1) : 0u;
+        if (__ldg(cdf + c) == prev) continue;  // zero weight
+        int lo, hi;
+        combo_cards(c, lo, hi);
+        if (!(used & ((1ull << lo) | (1ull << hi)))) pick = c;
+      }
+      if (pick < 0) pick = start;  // range exhausted by card removal: keep the draw
+      combo[p] = pick;
+      int lo, hi;
+      combo_cards(pick, lo, hi);
+      used |= (1ull << lo) | (1ull << hi);
+    }
+  }
+  DealRec r;
+  for (int i = 0; i < 10; ++i) r.pad[i] = 0;
+  for (int i = 0; i < 5; ++i) r.board[i] = (i < nb) ? G.sub_board[i] : 0;
+  int river = -1;
+  if (nb == 4) {
+    const U4 w = philox(U4{t, uid, 0x200u, 0u}, G.seed_lo, G.seed_hi);
+    const int free_cards = 52 - __popcll(used);
+    int k = (int)(((unsigned long long)w.x * (unsigned long long)free_cards) >> 32);
+    for (int c = 0; c < 52; ++c) {
+      if ((used >> c) & 1) continue;
+      if (k-- == 0) {
+        river = c;
+        break;
+      }
+    }
+    r.board[4] = (uint8_t)river;
+  }
+  r.dealer = (uint8_t)(N - 1);
+  int32_t b = __ldg(T + 53 + to_rm(r.board[0]));
+  for (int i = 1; i < 5; ++i) b = __ldg(T + b + to_rm(r.board[i]));
+  for (int p = 0; p < kMaxPlayers; ++p) {
+    r.ctx[p] = 0;
+    r.rank[p] = 0;
+    r.hole[2 * p] = r.hole[2 * p + 1] = 0;
+    if (p >= N) continue;
+    int lo, hi;
+    combo_cards(combo[p], lo, hi);
+    r.hole[2 * p] = (uint8_t)lo;
+    r.hole[2 * p + 1] = (uint8_t)hi;
+    const int32_t s6 = __ldg(T + b + to_rm(lo));
+    r.rank[p] = (uint16_t)decode16((uint32_t)__ldg(T + s6 + to_rm(hi)) & 0xFFFF);
+    r.ctx[p] = (uint32_t)combo[p] | ((uint32_t)(river + 1) << 16);
+  }
+  const uint4* src = reinterpret_cast<const uint4*>(&r);
+  uint4* dst = reinterpret_cast<uint4*>(out);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) dst[i] = src[i];
+}
+
 // Deal, buckets and river ranks of traversal t of update `uid`
 // (cfr_gpu.cu:460-470, 476-489, 942-952, 963).  `pre` is the 52x52 preflop LUT
 // (shared or global memory), `cdf` the rank-CDF LUTs.
 __device__ __forceinline__ void deal_one(const GameParams& G, const int32_t* __restrict__ T, const uint8_t* pre,
                                          const uint8_t* __restrict__ cdf, uint32_t t, uint32_t uid,
                                          DealRec* __restrict__ out) {
+  if (G.sub_street) {
+    deal_subgame(G, T, t, uid, out);
+    return;
+  }
   const int N = G.N;
   const int n_deal = 2 * N + 5;
   uint32_t words[24];

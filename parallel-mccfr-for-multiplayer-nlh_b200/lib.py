@@ -80,6 +80,11 @@ class BatchStats(Structure):
                 ("traverse_ms", c_double), ("total_ms", c_double), ("reserved", c_int32 * 8)]
 
 
+class Subgame(Structure):
+    _fields_ = [("street", c_int32), ("pot", c_int32), ("board", c_uint8 * 5), ("pad", c_uint8 * 3),
+                ("ranges", c_void_p)]
+
+
 class Trace(Structure):
     _fields_ = [
         ("hole", c_uint8 * 12), ("board", c_uint8 * 5), ("dealer", c_uint8), ("n_actions", c_uint8),
@@ -131,6 +136,10 @@ SIGNATURES = {
     "mccfr_batch_train": (c_int, [c_void_p, c_longlong, c_int]),
     "mccfr_batch_autotune": (c_int, [c_void_p, c_int, c_void_p]),
     "mccfr_batch_get_stats": (c_int, [c_void_p, c_void_p]),
+    "mccfr_create_subgame": (c_int, [POINTER(Config), c_void_p, POINTER(c_void_p)]),
+    "mccfr_share_hand_table": (c_int, [c_void_p, c_void_p]),
+    "mccfr_batch_round": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
+    "mccfr_get_progress": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
 }
 EVAL7_STATIC_MAX_HANDS = 1 << 18
 

@@ -1,0 +1,210 @@
+"""Subgame re-solve serving with continuous batching.
+
+Requests are turn or river subgames (board, 2-6 players, pot, one 1326-combo
+range per player, bet sizes, iteration budget).  The server keeps every admitted
+request's regret table resident on the device and runs rounds: each round is
+one mccfr_batch_round call, i.e. one player-update of every active request in a
+single persistent traversal launch.  Requests that arrive while others run are
+admitted between rounds as soon as a slot and device memory are free, and a
+request retires (its strategy is copied to the host) as soon as its budget is
+spent, so solves overlap on the device.  A request's result depends only on its
+own tables and Philox keys, never on what it was batched with.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import lib as L
+from .trainer import GPUCFRTrainer, batch_round
+
+# Bet sizes as pot fractions (num, den): 0.33, 0.5, 0.75, 1, 1.5, 2.
+BET_SIZES = [(1, 3), (1, 2), (3, 4), (1, 1), (3, 2), (2, 1)]
+CHIPS_PER_BB = 100
+STACK_BB = 100
+
+
+def combo_index(a: int, b: int) -> int:
+    lo, hi = min(a, b), max(a, b)
+    return hi * (hi - 1) // 2 + lo
+
+
+def _combo_cards() -> np.ndarray:
+    out = np.zeros((1326, 2), dtype=np.int64)
+    for hi in range(1, 52):
+        for lo in range(hi):
+            out[combo_index(lo, hi)] = (lo, hi)
+    return out
+
+
+COMBO_CARDS = _combo_cards()
+
+
+@dataclass
+class Request:
+    rid: int
+    street: int                 # 2 turn, 3 river
+    board: list[int]
+    players: int
+    pot: int                    # chips, a multiple of players
+    ranges: np.ndarray          # [players][1326]
+    sizes: list[tuple[int, int]]
+    budget: int                 # traversals per player
+    arrival: float = 0.0        # seconds since the start of the trace
+    table_log2: int = 16
+
+
+def make_request(rng: np.random.Generator, rid: int, max_sizes: int = 5) -> Request:
+    """A request drawn as the re-solve workload specifies: uniform turn or river
+    board, 2-6 players, pot U[2,200] BB, Dirichlet(0.5) ranges with board-blocked
+    combos zeroed, 3-6 sizes from {0.33,0.5,0.75,1,1.5,2} pot plus all-in (at most
+    `max_sizes`: fold, check/call, the sizes and all-in must fit 8 action
+    slots), iteration budget log-uniform in [2e3, 5e4]."""
+    street = int(rng.choice([2, 3]))
+    players = int(rng.integers(2, 7))
+    board = [int(c) for c in rng.permutation(52)[: (4 if street == 2 else 5)]]
+    pot_bb = float(rng.uniform(2.0, 200.0))
+    pot = max(players, int(round(pot_bb * CHIPS_PER_BB / players)) * players)
+    blocked = np.isin(COMBO_CARDS, board).any(axis=1)
+    ranges = rng.dirichlet(np.full(1326, 0.5), size=players).astype(np.float64)
+    ranges[:, blocked] = 0.0
+    ranges /= ranges.sum(axis=1, keepdims=True)
+    k = int(rng.integers(3, 7))
+    k = min(k, max_sizes)
+    sizes = sorted(set(BET_SIZES[i] for i in rng.choice(6, size=k, replace=False)), key=lambda f: f[0] / f[1])
+    budget = int(round(math.exp(rng.uniform(math.log(2e3), math.log(5e4)))))
+    rows = budget * players * 64
+    table_log2 = int(min(21, max(14, math.ceil(math.log2(max(rows, 2))))))
+    return Request(rid, street, board, players, pot, ranges.astype(np.float32), sizes, budget,
+                   table_log2=table_log2)
+
+
+def request_config(req: Request) -> L.Config:
+    c = L.preset(L.PRESET_HU_20BB)
+    c.num_players = req.players
+    c.small_blind = CHIPS_PER_BB // 2
+    c.big_blind = CHIPS_PER_BB
+    c.starting_stack = STACK_BB * CHIPS_PER_BB
+    slots = [(L.ACT_FOLD, 0, 1), (L.ACT_CHECK_CALL, 0, 1)] + [(L.ACT_RAISE_POT, n, d) for n, d in req.sizes]
+    slots.append((L.ACT_ALL_IN, 0, 1))
+    c.num_actions = len(slots)
+    for a, (k, n, d) in enumerate(slots):
+        c.action_kind[a], c.action_num[a], c.action_den[a] = k, n, d
+    c.raise_cap = 2
+    c.max_depth = 255
+    c.table_log2 = req.table_log2
+    c.key_bits = req.table_log2 - 1
+    c.seed = 0x5EED0000 + req.rid
+    return c
+
+
+def table_bytes(req: Request) -> int:
+    return (1 << req.table_log2) * (256 + 4) + (1 << 20)
+
+
+@dataclass
+class Solve:
+    req: Request
+    trainer: GPUCFRTrainer
+    updates_needed: int
+    updates_done: int = 0
+    admitted: float = 0.0
+
+
+@dataclass
+class Result:
+    rid: int
+    arrival: float
+    admitted: float
+    finished: float
+    keys: np.ndarray = field(repr=False)
+    probs: np.ndarray = field(repr=False)
+
+    @property
+    def latency_ms(self) -> float:
+        return (self.finished - self.arrival) * 1e3
+
+
+class ReSolveServer:
+    """Continuous-batching re-solver.
+
+    hbm_budget: device bytes the server may hold in request tables (admission
+    also requires that much free device memory); max_active: requests batched
+    per round (the persistent kernel takes up to 64 tables); traversals: per
+    player-update of each request."""
+
+    def __init__(self, rank_table_owner: GPUCFRTrainer, hbm_budget: int = 16 << 30, max_active: int = 64,
+                 traversals: int = 256, tuning: dict | None = None, free_memory=None):
+        self.owner = rank_table_owner
+        self.hbm_budget = int(hbm_budget)
+        self.max_active = min(64, int(max_active))
+        self.traversals = int(traversals)
+        self.tuning = tuning
+        self.free_memory = free_memory or self._device_free
+        self.rounds = 0
+
+    @staticmethod
+    def _device_free() -> int:
+        import torch
+
+        return int(torch.cuda.mem_get_info()[0])
+
+    def admit_ok(self, req: Request, held: int, n_active: int) -> bool:
+        need = table_bytes(req)
+        return n_active < self.max_active and held + need <= self.hbm_budget and need + (1 << 30) <= self.free_memory()
+
+    def _start(self, req: Request, now: float) -> Solve:
+        t = GPUCFRTrainer.subgame(request_config(req), req.street, req.pot, req.board, req.ranges)
+        t.share_hand_table(self.owner)
+        per_player = max(1, math.ceil(req.budget / self.traversals))
+        return Solve(req, t, per_player * req.players, admitted=now)
+
+    def run(self, requests: list[Request], realtime: bool = True) -> list[Result]:
+        """Serves requests in arrival order; with realtime=False arrivals are
+        ignored and every request is available at once."""
+        pending = sorted(requests, key=lambda r: r.arrival)
+        queue: list[Request] = []
+        active: list[Solve] = []
+        held = 0
+        results: list[Result] = []
+        t0 = time.perf_counter()
+        while pending or queue or active:
+            now = time.perf_counter() - t0
+            while pending and (not realtime or pending[0].arrival <= now):
+                queue.append(pending.pop(0))
+            while queue and self.admit_ok(queue[0], held, len(active)):
+                req = queue.pop(0)
+                active.append(self._start(req, time.perf_counter() - t0))
+                held += table_bytes(req)
+            if not active:
+                if pending:
+                    time.sleep(max(0.0, min(0.001, pending[0].arrival - now)))
+                continue
+            batch_round([s.trainer for s in active], [self.traversals] * len(active), self.tuning)
+            self.rounds += 1
+            still = []
+            for s in active:
+                s.updates_done += 1
+                if s.updates_done >= s.updates_needed:
+                    keys, probs = s.trainer.strategy_arrays()
+                    results.append(Result(s.req.rid, s.req.arrival, s.admitted, time.perf_counter() - t0, keys, probs))
+                    s.trainer.close()
+                    held -= table_bytes(s.req)
+                else:
+                    still.append(s)
+            active = still
+        return results
+
+
+def poisson_arrivals(rng: np.random.Generator, n: int, rate: float) -> np.ndarray:
+    return np.cumsum(rng.exponential(1.0 / rate, size=n))
+
+
+def summarize(results: list[Result]) -> dict:
+    lat = np.array([r.latency_ms for r in results])
+    span = max(r.finished for r in results) - min(r.arrival for r in results)
+    return {"requests": len(results), "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()), "solves_per_s": len(results) / span}

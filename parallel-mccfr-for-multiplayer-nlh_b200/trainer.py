@@ -50,6 +50,34 @@ class GPUCFRTrainer:
         self._h = h
         self.iterations_done = 0
 
+    @classmethod
+    def subgame(cls, config: L.Config, street: int, pot: int, board, ranges: np.ndarray) -> "GPUCFRTrainer":
+        """A turn (street 2, 4 board cards) or river (street 3, 5 cards) subgame with
+        one 1326-combo range per player (mccfr_create_subgame)."""
+        self = cls.__new__(cls)
+        self._lib = L.load()
+        self.config = config
+        r = np.ascontiguousarray(ranges, dtype=np.float32).reshape(config.num_players, 1326)
+        sg = L.Subgame()
+        sg.street = int(street)
+        sg.pot = int(pot)
+        for i, c in enumerate(list(board)[:5]):
+            sg.board[i] = int(c)
+        sg.ranges = r.ctypes.data
+        h = c_void_p()
+        L.check(self._lib.mccfr_create_subgame(byref(config), byref(sg), byref(h)))
+        self._h = h
+        self.iterations_done = 0
+        return self
+
+    def share_hand_table(self, src: "GPUCFRTrainer") -> None:
+        L.check(self._lib.mccfr_share_hand_table(self._h, src.handle), self._h)
+
+    def progress(self) -> tuple[int, int, int]:
+        it, pl, done = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_longlong()
+        L.check(self._lib.mccfr_get_progress(self._h, byref(it), byref(pl), byref(done)), self._h)
+        return it.value, pl.value, done.value
+
     # -- lifetime ------------------------------------------------------------
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -225,3 +253,16 @@ class Batch:
         s = L.BatchStats()
         L.check(self._lib.mccfr_batch_get_stats(self._b, byref(s)))
         return s
+
+
+def batch_round(trainers: list, traversals: list[int], tuning: dict | None = None) -> None:
+    """One player-update of every listed trainer in one persistent launch
+    (continuous batching step, mccfr_batch_round)."""
+    lib = L.load()
+    arr = (ctypes.c_void_p * len(trainers))(*[t.handle.value for t in trainers])
+    cnt = (ctypes.c_int * len(traversals))(*[int(x) for x in traversals])
+    tp = None
+    if tuning:
+        tp = byref(L.BatchTuning(tuning.get("block", 128), tuning.get("grab", 1), tuning.get("smem_frames", 0),
+                                 tuning.get("probe_width", 1), tuning.get("warp_sync", 1)))
+    L.check(lib.mccfr_batch_round(arr, len(trainers), cnt, tp))

@@ -1,0 +1,55 @@
+"""Host logic of the re-solve server (CPU): request generation and admission."""
+from __future__ import annotations
+
+import importlib
+
+import numpy as np
+
+from conftest import mccfr  # noqa: F401  (registers mccfr_b200)
+
+sv = importlib.import_module("mccfr_b200.serving")
+
+
+def test_requests_follow_the_workload():
+    rng = np.random.default_rng(0)
+    for rid in range(200):
+        r = sv.make_request(rng, rid)
+        assert r.street in (2, 3) and len(r.board) == (4 if r.street == 2 else 5)
+        assert len(set(r.board)) == len(r.board)
+        assert 2 <= r.players <= 6 and r.pot % r.players == 0
+        assert 2 * 100 - r.players <= r.pot <= 200 * 100 + r.players
+        assert r.ranges.shape == (r.players, 1326)
+        blocked = np.isin(sv.COMBO_CARDS, r.board).any(axis=1)
+        assert np.all(r.ranges[:, blocked] == 0)
+        assert np.allclose(r.ranges.sum(1), 1.0, atol=1e-5)
+        assert 3 <= len(r.sizes) <= 5 and all(s in sv.BET_SIZES for s in r.sizes)
+        assert 2000 <= r.budget <= 50000
+        assert 14 <= r.table_log2 <= 21
+        c = sv.request_config(r)
+        assert c.num_actions == len(r.sizes) + 3 <= 8
+
+
+def test_combo_index_is_a_bijection():
+    seen = {sv.combo_index(a, b) for a in range(52) for b in range(a + 1, 52)}
+    assert seen == set(range(1326))
+    for i, (lo, hi) in enumerate(sv.COMBO_CARDS):
+        assert sv.combo_index(lo, hi) == i
+
+
+def test_admission_respects_budget_and_free_memory():
+    rng = np.random.default_rng(1)
+    req = sv.make_request(rng, 0)
+    need = sv.table_bytes(req)
+    srv = sv.ReSolveServer(None, hbm_budget=3 * need, max_active=2, free_memory=lambda: 100 << 30)
+    assert srv.admit_ok(req, 0, 0)
+    assert not srv.admit_ok(req, 0, 2)          # slots
+    assert not srv.admit_ok(req, 3 * need, 0)   # budget
+    tight = sv.ReSolveServer(None, hbm_budget=1 << 40, free_memory=lambda: need)
+    assert not tight.admit_ok(req, 0, 0)        # device memory
+
+
+def test_poisson_arrivals_rate():
+    rng = np.random.default_rng(2)
+    a = sv.poisson_arrivals(rng, 20000, 100.0)
+    assert np.all(np.diff(a) > 0)
+    assert abs(20000 / a[-1] - 100.0) < 3.0
