@@ -271,6 +271,32 @@ def multitable(m, L, table, iters=2) -> dict:
                         "LogNormal(14,1)/16, seed 2; wall clock over 2 iterations after warm-up"}
 
 
+def serving_sweep(m, L, table, rates=(10, 30, 100, 300, 1000), n_requests=48) -> dict:
+    """Re-solve serving at several Poisson arrival rates: p50/p99 latency (arrival
+    to strategy on the host) and solves/s, continuous batching on one B200."""
+    import importlib
+
+    import numpy as np
+
+    sv = importlib.import_module("mccfr_b200.serving")
+    owner = m.GPUCFRTrainer(config=L.preset(L.PRESET_HU_20BB), table_log2=10)
+    owner.set_hand_table(table)
+    out = {}
+    for rate in rates:
+        rng = np.random.default_rng(4)
+        reqs = [sv.make_request(rng, i) for i in range(n_requests)]
+        for r, a in zip(reqs, sv.poisson_arrivals(rng, n_requests, rate)):
+            r.arrival = float(a)
+        srv = sv.ReSolveServer(owner, hbm_budget=32 << 30, traversals=1024)
+        res = srv.run(reqs)
+        out[f"lambda_{rate}"] = {**sv.summarize(res), "rounds": srv.rounds}
+    owner.close()
+    out["workload"] = (f"{n_requests} requests per rate: turn/river board, 2-6 players, pot U[2,200]BB, "
+                       "Dirichlet(0.5) ranges, 3-5 sizes + all-in, budget log-uniform [2e3,5e4] traversals per "
+                       "player, 1024 traversals per update, 100BB stacks, seed 4")
+    return out
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -411,6 +437,7 @@ def main():
         extras = {}
         extras["batched_same_table"] = batched_same_table(m, L, table, args, value)
         extras["c3_multitable"] = multitable(m, L, table)
+        extras["resolve_serving"] = serving_sweep(m, L, table)
         for wl in ("ref8-6max", "6max-100bb-refrule"):
             if wl == args.workload:
                 continue

@@ -1617,6 +1617,7 @@ struct RoundCtx {
   DealRec* d_deals = nullptr;
   unsigned long long* d_work = nullptr;
   size_t deals_cap = 0;
+  int* h_err = nullptr;  // pinned: the tables' error flags after a round
   PhaseParams params;
 };
 
@@ -1746,6 +1747,7 @@ int mccfr_batch_round(mccfr_handle* const* tables, int n, const int* traversals,
     BCK(cudaMalloc(&R.d_tables, kMaxBatchTables * sizeof(TableDesc)));
     BCK(cudaMalloc(&R.d_phase, sizeof(PhaseDesc)));
     BCK(cudaMalloc(&R.d_work, sizeof(unsigned long long)));
+    BCK(cudaMallocHost(&R.h_err, kMaxBatchTables * sizeof(int)));
     R.device = dev;
   }
   unsigned long long total = 0;
@@ -1810,6 +1812,8 @@ int mccfr_batch_round(mccfr_handle* const* tables, int n, const int* traversals,
   k_apply_batched<<<dim3(std::max(1, std::min(148 * 2, (int)((off * 8 + 255) / 256) + 1)), n), 256, 0, R.stream>>>(
       R.d_tables, R.d_phase);
   BCK(cudaGetLastError());
+  for (int i = 0; i < n; ++i)  // every table's error flag in one synchronisation
+    BCK(cudaMemcpyAsync(R.h_err + i, tables[i]->tv.err, sizeof(int), cudaMemcpyDeviceToHost, R.stream));
   BCK(cudaStreamSynchronize(R.stream));
   int worst = MCCFR_OK;
   for (int i = 0; i < n; ++i) {
@@ -1819,8 +1823,10 @@ int mccfr_batch_round(mccfr_handle* const* tables, int n, const int* traversals,
       h->round_player = 0;
       h->iterations_done++;
     }
-    const int rc = check_device_error(h);
-    if (rc && !worst) worst = rc;
+    if (R.h_err[i]) {
+      const int rc = check_device_error(h);
+      if (rc && !worst) worst = rc;
+    }
   }
   return worst;
 }
