@@ -285,7 +285,8 @@ int mccfr_batch_get_stats(mccfr_batch* b, mccfr_batch_stats* out);
    cards lo < hi is index hi*(hi-1)/2 + lo; combos that use a board card get
    weight 0).  Hole combos are drawn from the ranges with card removal; info
    sets are keyed by the exact combo (and the river card on the river).  The
-   subgame uses external sampling and 64-bit keys. */
+   subgame uses 64-bit keys; either update rule.  The batched form and the
+   round API run external sampling only. */
 typedef struct mccfr_subgame {
   int32_t street;         /* 2 = turn (4 board cards), 3 = river (5) */
   int32_t pot;            /* chips in the pot; must be a multiple of num_players */
@@ -323,6 +324,57 @@ int mccfr_get_progress(mccfr_handle* h, long long* next_iteration, int* next_pla
    calls that overlap on the GPU race: serialise them. */
 #define MCCFR_EVAL7_STATIC_MAX_HANDS (1u << 18)
 int mccfr_eval7_static(const int32_t* dev_table, const uint8_t* cards, uint16_t* ranks, size_t n);
+
+/* ---- heads-up best response and exploitability -------------------------
+   No counterpart in the reference (its PROPOSAL.md:99 calls exploitability too
+   expensive; play is judged against scripted bots).  An exact best response
+   in double precision on host threads, for heads-up games only: the full game
+   from the blinds (rank-CDF postflop buckets, which are suit-invariant, so
+   flops are enumerated up to suit permutation), or a turn/river subgame.  The
+   evaluated strategy is the rows' strategy sums normalised over each node's
+   legal slots; a missing row, or one whose legal sum is 0, plays uniformly.
+   The best responder plays the real game: it sees its own cards, the board
+   and the action history.  Chance follows the trainer's deal: uniform hole
+   cards and a uniform dealer in the full game; in a subgame the hole combos
+   drawn with probability proportional to the product of the quantised range
+   weights over disjoint pairs (the deal's accepted draw), then a uniform
+   river card. */
+#define MCCFR_BR_VERBOSE 1   /* progress on stderr */
+#define MCCFR_BR_ISO_CHECK 2 /* full game: recompute some suit-permuted flops directly */
+typedef struct mccfr_br_options {
+  int32_t threads;      /* host threads; 0 = all */
+  int32_t flop_stride;  /* full game: 1 = every flop class (exact); k > 1 = every
+                           k-th class, reweighted (an estimate, exact = 0) */
+  int32_t flags;
+  int32_t reserved[5];
+} mccfr_br_options;
+typedef struct mccfr_exploit {
+  double br_value[2];       /* chips per game: player p best-responding to the other */
+  double profile_value[2];  /* chips per game: the average-strategy profile, player p */
+  double exploitability;    /* (br_value[0] + br_value[1]) / 2, chips per game */
+  double mbb_per_game;      /* exploitability in milli-big-blinds per game */
+  double seconds;           /* host time of the computation */
+  double iso_check;         /* MCCFR_BR_ISO_CHECK: largest difference found, relative to the
+                               largest value of the flop compared; else 0 */
+  long long boards;         /* river boards evaluated (flop classes count once) */
+  long long rows;           /* strategy rows supplied */
+  long long nodes;          /* public-tree nodes (all dealer seats) */
+  int32_t threads;
+  int32_t exact;
+  int32_t reserved[4];
+} mccfr_exploit;
+void mccfr_br_options_init(mccfr_br_options* opt);
+/* From host data: cfg (num_players 2), sg NULL for the full game, the rank
+   table, and rows as mccfr_export_rows writes them (keys, strategy_sum [rows][8]). */
+int mccfr_best_response(const mccfr_config* cfg, const mccfr_subgame* sg, const int32_t* hand_table,
+                        size_t table_entries, const uint64_t* keys, const float* strategy_sum, size_t rows,
+                        const mccfr_br_options* opt, mccfr_exploit* out);
+/* The same for a trainer's current average strategy (its rows and rank table
+   are copied from the device). */
+int mccfr_exploitability(mccfr_handle* h, const mccfr_br_options* opt, mccfr_exploit* out);
+/* Rank-CDF bucket LUT of n-card hands (n = 5, 6, 7) from the exact rank
+   histogram, as the trainer builds it: out[rank] for rank 0..7462. */
+int mccfr_rank_cdf_lut(const int32_t* hand_table, size_t table_entries, int ncards, int buckets, uint8_t* out);
 
 #ifdef __cplusplus
 }

@@ -20,8 +20,8 @@ LIB = PKG / "libmccfr.so"
 ORACLE_DIR = ROOT / "oracle"
 REFERENCE_SRC = Path("/root/reference/poker_cuda/src")
 
-SOURCES = ["mccfr.cu", "eval_static.cu", "handtable.cpp", "abstraction.cpp"]
-HEADERS = ["game.cuh", "table.cuh", "traverse_ref.cuh", "traverse_es.cuh", "batched.cuh", "handtable.h"]
+SOURCES = ["mccfr.cu", "eval_static.cu", "best_response.cu", "handtable.cpp", "abstraction.cpp"]
+HEADERS = ["game.cuh", "table.cuh", "traverse_ref.cuh", "traverse_es.cuh", "batched.cuh", "handtable.h", "best_response.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

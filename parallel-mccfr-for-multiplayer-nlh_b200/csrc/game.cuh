@@ -63,12 +63,12 @@ __device__ __forceinline__ float uniform01(uint32_t w) {
 
 constexpr uint64_t kPathSeed = 0x243F6A8885A308D3ull;
 
-__device__ __forceinline__ uint64_t path_step(uint64_t h, int a) {
+__host__ __device__ __forceinline__ uint64_t path_step(uint64_t h, int a) {
   h = (h ^ (uint64_t)(a + 1)) * 0x9E3779B97F4A7C15ull;
   return h ^ (h >> 31);
 }
 
-__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
   z ^= z >> 33;
   z *= 0xFF51AFD7ED558CCDull;
   z ^= z >> 33;
@@ -80,9 +80,9 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
 // ---------------------------------------------------------------------------
 // Rank table helpers (cfr_gpu.cu:87-112).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int to_rm(int c) { return (c % 13) * 4 + c / 13 + 1; }
+__host__ __device__ __forceinline__ int to_rm(int c) { return (c % 13) * 4 + c / 13 + 1; }
 
-__device__ __forceinline__ uint32_t decode16(uint32_t packed16) {
+__host__ __device__ __forceinline__ uint32_t decode16(uint32_t packed16) {
   const uint32_t cat = (packed16 >> 12) & 0xF;
   const uint32_t ord = packed16 & 0x0FFFu;
   if (ord == 0 || cat < 1 || cat > 9) return 0;
@@ -103,17 +103,20 @@ __device__ __forceinline__ uint32_t ref_linear_bucket(uint32_t rank16, int bucke
 // Action rules (cfr_gpu.cu:186-244, abstraction.cpp:144-234) with an optional
 // per-street raise cap.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int min_raise_to(int cb, int lfr, int bb) {
-  return (cb == 0) ? max(1, bb) : cb + max(lfr, bb);
+__host__ __device__ __forceinline__ int imax(int a, int b) { return a > b ? a : b; }
+__host__ __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
+
+__host__ __device__ __forceinline__ int min_raise_to(int cb, int lfr, int bb) {
+  return (cb == 0) ? imax(1, bb) : cb + imax(lfr, bb);
 }
 
-__device__ __forceinline__ int raise_target(const GameParams& G, int a, int pot, int cb, int mrt) {
+__host__ __device__ __forceinline__ int raise_target(const GameParams& G, int a, int pot, int cb, int mrt) {
   if (G.kind[a] == 4 /*RAISE_MIN*/) return mrt;
   const int frac = (G.num[a] * pot) / G.den[a];
-  return max(mrt, cb + max(1, frac));
+  return imax(mrt, cb + imax(1, frac));
 }
 
-__device__ __forceinline__ uint32_t valid_mask(const GameParams& G, int pot, int stack, int to_call,
+__host__ __device__ __forceinline__ uint32_t valid_mask(const GameParams& G, int pot, int stack, int to_call,
                                                int cb, int lfr, int raises) {
   if (pot <= 0) pot = 1;
   uint32_t m;
@@ -138,17 +141,17 @@ __device__ __forceinline__ uint32_t valid_mask(const GameParams& G, int pot, int
   return m | G.m_allin;
 }
 
-__device__ __forceinline__ int chips_for(const GameParams& G, int a, int pot, int stack, int to_call,
-                                         int cb, int lfr) {
+__host__ __device__ __forceinline__ int chips_for(const GameParams& G, int a, int pot, int stack, int to_call,
+                                                  int cb, int lfr) {
   if (pot <= 0) pot = 1;
   const int k = G.kind[a];
   if (k == 0 || k == 1) return 0;             // fold, check
-  if (k == 2 || k == 3) return min(to_call, stack);  // call, check/call
+  if (k == 2 || k == 3) return imin(to_call, stack);  // call, check/call
   if (k == 6) return stack;                   // all-in
   const int mrt = min_raise_to(cb, lfr, G.bb);
-  const int maxrt = cb + max(0, stack - to_call);
-  const int t = min(raise_target(G, a, pot, cb, mrt), maxrt);
-  return min(to_call + max(0, t - cb), stack);
+  const int maxrt = cb + imax(0, stack - to_call);
+  const int t = imin(raise_target(G, a, pot, cb, mrt), maxrt);
+  return imin(to_call + imax(0, t - cb), stack);
 }
 
 __device__ __forceinline__ int passive_fallback(const GameParams& G, uint32_t vm) {
@@ -224,7 +227,7 @@ __device__ __forceinline__ void combo_cards(int idx, int& lo, int& hi) {
 }
 
 // Reference info-set slot (cfr_gpu.cu:165-179).
-__device__ __forceinline__ uint32_t fnv_slot(uint32_t player, uint32_t hb, uint32_t bb,
+__host__ __device__ __forceinline__ uint32_t fnv_slot(uint32_t player, uint32_t hb, uint32_t bb,
                                              uint32_t street, uint32_t bits) {
   uint32_t h = 2166136261u;
   h = (h ^ (player & 0xFF)) * 16777619u;
@@ -238,7 +241,7 @@ __device__ __forceinline__ uint32_t fnv_slot(uint32_t player, uint32_t hb, uint3
   return h & ((1u << 26) - 1);
 }
 
-__device__ __forceinline__ uint64_t info_key(const GameParams& G, uint32_t player, uint32_t hb,
+__host__ __device__ __forceinline__ uint64_t info_key(const GameParams& G, uint32_t player, uint32_t hb,
                                              uint32_t bb, uint32_t street, uint32_t abits,
                                              uint64_t path) {
   if (G.key_mode == 0) return (uint64_t)fnv_slot(player, hb, bb, street, abits) + 1;

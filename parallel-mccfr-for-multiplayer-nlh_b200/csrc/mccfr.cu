@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -31,6 +32,7 @@
 #include "traverse_ref.cuh"
 #include "traverse_es.cuh"
 #include "batched.cuh"
+#include "best_response.h"
 
 namespace mccfr {
 void build_preflop_lut(int mode, int buckets, uint8_t* lut);
@@ -1661,8 +1663,8 @@ extern "C" {
 
 int mccfr_create_subgame(const mccfr_config* cfg, const mccfr_subgame* sg, mccfr_handle** out) {
   if (!cfg || !sg || !out || !sg->ranges) return MCCFR_ERR_INVALID_ARG;
-  if (cfg->sampling != MCCFR_SAMPLING_EXTERNAL || cfg->key_mode != MCCFR_KEY_ID64) {
-    fprintf(stderr, "mccfr_create_subgame: subgames use external sampling and ID64 keys\n");
+  if (cfg->key_mode != MCCFR_KEY_ID64) {
+    fprintf(stderr, "mccfr_create_subgame: subgames use ID64 keys\n");
     return MCCFR_ERR_INVALID_ARG;
   }
   if (sg->street != 2 && sg->street != 3) return MCCFR_ERR_INVALID_ARG;
@@ -1829,6 +1831,116 @@ int mccfr_batch_round(mccfr_handle* const* tables, int n, const int* traversals,
     }
   }
   return worst;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Heads-up best response (host engine in best_response.cu).
+// ---------------------------------------------------------------------------
+extern "C" {
+
+void mccfr_br_options_init(mccfr_br_options* opt) {
+  if (!opt) return;
+  std::memset(opt, 0, sizeof(*opt));
+  opt->flop_stride = 1;
+}
+
+int mccfr_rank_cdf_lut(const int32_t* hand_table, size_t table_entries, int ncards, int buckets, uint8_t* out) {
+  if (!hand_table || !out || table_entries != (size_t)MCCFR_HAND_TABLE_ENTRIES || ncards < 5 || ncards > 7 ||
+      buckets < 1 || buckets > 256)
+    return MCCFR_ERR_INVALID_ARG;
+  unsigned long long hist[7463];
+  host_rank_hist(hand_table, ncards, hist, 0 + (int)std::max(1u, std::thread::hardware_concurrency()));
+  build_cdf_lut(hist, buckets, out);
+  return MCCFR_OK;
+}
+
+int mccfr_best_response(const mccfr_config* cfg, const mccfr_subgame* sg, const int32_t* hand_table,
+                        size_t table_entries, const uint64_t* keys, const float* strategy_sum, size_t rows,
+                        const mccfr_br_options* opt, mccfr_exploit* out) {
+  if (!cfg || !hand_table || !out || (rows && (!keys || !strategy_sum))) return MCCFR_ERR_INVALID_ARG;
+  if (table_entries != (size_t)MCCFR_HAND_TABLE_ENTRIES) return MCCFR_ERR_FORMAT;
+  std::string why;
+  if (validate(*cfg, why)) {
+    fprintf(stderr, "mccfr_best_response: %s\n", why.c_str());
+    return MCCFR_ERR_INVALID_ARG;
+  }
+  mccfr_br_options o;
+  mccfr_br_options_init(&o);
+  if (opt) o = *opt;
+  GameParams g;
+  make_params(*cfg, g);
+  BrInput in;
+  in.cfg = cfg;
+  in.T = hand_table;
+  in.keys = keys;
+  in.ssum = strategy_sum;
+  in.rows = rows;
+  if (sg) {
+    if (!sg->ranges || (sg->street != 2 && sg->street != 3) || cfg->num_players != 2) return MCCFR_ERR_INVALID_ARG;
+    const int nb = sg->street == 2 ? 4 : 5;
+    uint64_t mask = 0;
+    for (int i = 0; i < nb; ++i) {
+      if (sg->board[i] > 51 || ((mask >> sg->board[i]) & 1)) return MCCFR_ERR_INVALID_ARG;
+      mask |= 1ull << sg->board[i];
+    }
+    if (sg->pot < 0 || sg->pot % 2 != 0) return MCCFR_ERR_INVALID_ARG;
+    g.sub_street = sg->street;
+    g.sub_pot = sg->pot;
+    for (int i = 0; i < 5; ++i) g.sub_board[i] = (i < nb) ? sg->board[i] : 0;
+    for (int p = 0; p < 2; ++p) {
+      uint32_t cdf[1326];
+      if (!build_range_cdf(sg->ranges + 1326 * p, mask, cdf)) return MCCFR_ERR_INVALID_ARG;
+      in.weights[p].resize(1326);
+      for (int c = 0; c < 1326; ++c) in.weights[p][c] = (double)cdf[c] - (c ? (double)cdf[c - 1] : 0.0);
+    }
+  }
+  in.G = &g;
+  std::string err;
+  const int rc = run_best_response(in, o, out, err);
+  if (rc) fprintf(stderr, "mccfr_best_response: %s\n", err.c_str());
+  return rc;
+}
+
+int mccfr_exploitability(mccfr_handle* h, const mccfr_br_options* opt, mccfr_exploit* out) {
+  if (!h || !out) return MCCFR_ERR_INVALID_ARG;
+  if (!h->has_table) return fail(h, MCCFR_ERR_NO_HAND_TABLE, "no hand table loaded");
+  CK(cudaSetDevice(h->device));
+  std::vector<HostRow> rows;
+  int rc = read_rows(h, rows);
+  if (rc) return rc;
+  std::vector<uint64_t> keys(rows.size());
+  std::vector<float> ssum(rows.size() * 8);
+  for (size_t i = 0; i < rows.size(); ++i) {
+    keys[i] = rows[i].key;
+    std::memcpy(&ssum[8 * i], rows[i].ssum, 32);
+  }
+  std::vector<int32_t> table(MCCFR_HAND_TABLE_ENTRIES);
+  CK(cudaMemcpy(table.data(), h->d_hr, table.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  mccfr_br_options o;
+  mccfr_br_options_init(&o);
+  if (opt) o = *opt;
+  BrInput in;
+  in.cfg = &h->cfg;
+  in.G = &h->gp;
+  in.T = table.data();
+  in.keys = keys.data();
+  in.ssum = ssum.data();
+  in.rows = rows.size();
+  if (h->gp.sub_street) {
+    std::vector<uint32_t> cdf(2 * 1326);
+    CK(cudaMemcpy(cdf.data(), h->d_ranges, cdf.size() * 4, cudaMemcpyDeviceToHost));
+    for (int p = 0; p < 2; ++p) {
+      in.weights[p].resize(1326);
+      for (int c = 0; c < 1326; ++c)
+        in.weights[p][c] = (double)cdf[1326 * p + c] - (c ? (double)cdf[1326 * p + c - 1] : 0.0);
+    }
+  }
+  std::string err;
+  rc = run_best_response(in, o, out, err);
+  if (rc) return fail(h, rc, "%s", err.c_str());
+  return MCCFR_OK;
 }
 
 }  // extern "C"

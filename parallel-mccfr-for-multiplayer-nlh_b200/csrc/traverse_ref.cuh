@@ -355,28 +355,38 @@ k_traverse_ref(const GameParams G, const TableView tv, const DealRec* __restrict
       s_inv[p][tid] = 0;
     }
 
-  // Blinds and preflop queue (cfr_gpu.cu:954-981).
+  // Blinds and preflop queue (cfr_gpu.cu:954-981), or a subgame's start.
   int pot, cb, lfr = G.bb, raises = 0, street = 0;
   uint32_t folded = 0, allin = 0, abits = 0;
   uint64_t path = kPathSeed;
-  const int sbp = (N == 2) ? dealer : (dealer + 1) % N;
-  const int bbp = (N == 2) ? (dealer + 1) % N : (dealer + 2) % N;
-  const int sba = min(G.sb, G.stack), bba = min(G.bb, G.stack);
-  s_stack[sbp][tid] = (uint16_t)(G.stack - sba);
-  s_bet[sbp][tid] = (uint16_t)sba;
-  s_inv[sbp][tid] = (uint16_t)sba;
-  s_stack[bbp][tid] = (uint16_t)(G.stack - bba);
-  s_bet[bbp][tid] = (uint16_t)bba;
-  s_inv[bbp][tid] = (uint16_t)bba;
-  pot = sba + bba;
-  cb = bba;
-  if (G.stack - sba == 0) allin |= 1u << sbp;
-  if (G.stack - bba == 0) allin |= 1u << bbp;
   uint32_t q = 0;  // action queue, 4-bit entries
   int nq = 0;
-  for (int i = 0; i < N; ++i) {
-    const int p = (bbp + 1 + i) % N;
-    if (!((allin >> p) & 1)) q |= (uint32_t)p << (4 * nq++);
+  if (G.sub_street) {
+#pragma unroll
+    for (int p = 0; p < kMaxPlayers; ++p)
+      if (p < N) s_inv[p][tid] = (uint16_t)(G.sub_pot / N);
+    pot = G.sub_pot;
+    cb = 0;
+    street = G.sub_street;
+    for (int i = 1; i <= N; ++i) q |= (uint32_t)((dealer + i) % N) << (4 * nq++);
+  } else {
+    const int sbp = (N == 2) ? dealer : (dealer + 1) % N;
+    const int bbp = (N == 2) ? (dealer + 1) % N : (dealer + 2) % N;
+    const int sba = min(G.sb, G.stack), bba = min(G.bb, G.stack);
+    s_stack[sbp][tid] = (uint16_t)(G.stack - sba);
+    s_bet[sbp][tid] = (uint16_t)sba;
+    s_inv[sbp][tid] = (uint16_t)sba;
+    s_stack[bbp][tid] = (uint16_t)(G.stack - bba);
+    s_bet[bbp][tid] = (uint16_t)bba;
+    s_inv[bbp][tid] = (uint16_t)bba;
+    pot = sba + bba;
+    cb = bba;
+    if (G.stack - sba == 0) allin |= 1u << sbp;
+    if (G.stack - bba == 0) allin |= 1u << bbp;
+    for (int i = 0; i < N; ++i) {
+      const int p = (bbp + 1 + i) % N;
+      if (!((allin >> p) & 1)) q |= (uint32_t)p << (4 * nq++);
+    }
   }
 
   int nrec = 0;
@@ -431,8 +441,14 @@ k_traverse_ref(const GameParams G, const TableView tv, const DealRec* __restrict
     const int to_call = cb - pbet;
     const uint32_t vm = valid_mask(G, pot, pstack, to_call, cb, lfr, raises);
     const uint32_t cw = s_ctx[player][tid];
-    const uint32_t hb = cw & 0xFF;
-    const uint32_t bkt = street ? ((cw >> (8 * street)) & 0xFF) : 0u;
+    uint32_t hb, bkt;
+    if (G.sub_street) {  // exact combo; the river card once it is dealt
+      hb = cw & 0xFFFF;
+      bkt = (street == 3 && G.sub_street == 2) ? (cw >> 16) : 0u;
+    } else {
+      hb = cw & 0xFF;
+      bkt = street ? ((cw >> (8 * street)) & 0xFF) : 0u;
+    }
     const unsigned long long key = info_key(G, player, hb, bkt, street, abits, path);
     const bool is_up = (player == up);
     const long long slot = is_up ? table_insert(tv, key) : table_find(tv, key);

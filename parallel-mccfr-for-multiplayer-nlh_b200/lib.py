@@ -85,6 +85,26 @@ class Subgame(Structure):
                 ("ranges", c_void_p)]
 
 
+class BrOptions(Structure):
+    _fields_ = [("threads", c_int32), ("flop_stride", c_int32), ("flags", c_int32), ("reserved", c_int32 * 5)]
+
+
+BR_VERBOSE, BR_ISO_CHECK = 1, 2
+
+
+class Exploit(Structure):
+    _fields_ = [("br_value", c_double * 2), ("profile_value", c_double * 2), ("exploitability", c_double),
+                ("mbb_per_game", c_double), ("seconds", c_double), ("iso_check", c_double),
+                ("boards", c_longlong), ("rows", c_longlong), ("nodes", c_longlong), ("threads", c_int32),
+                ("exact", c_int32), ("reserved", c_int32 * 4)]
+
+    def as_dict(self) -> dict:
+        return {"br_value": list(self.br_value), "profile_value": list(self.profile_value),
+                "exploitability": self.exploitability, "mbb_per_game": self.mbb_per_game,
+                "seconds": self.seconds, "iso_check": self.iso_check, "boards": self.boards, "rows": self.rows,
+                "nodes": self.nodes, "threads": self.threads, "exact": bool(self.exact)}
+
+
 class Trace(Structure):
     _fields_ = [
         ("hole", c_uint8 * 12), ("board", c_uint8 * 5), ("dealer", c_uint8), ("n_actions", c_uint8),
@@ -140,6 +160,11 @@ SIGNATURES = {
     "mccfr_share_hand_table": (c_int, [c_void_p, c_void_p]),
     "mccfr_batch_round": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
     "mccfr_get_progress": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mccfr_br_options_init": (None, [c_void_p]),
+    "mccfr_best_response": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p, c_size_t,
+                                    c_void_p, c_void_p]),
+    "mccfr_exploitability": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "mccfr_rank_cdf_lut": (c_int, [c_void_p, c_size_t, c_int, c_int, c_void_p]),
 }
 EVAL7_STATIC_MAX_HANDS = 1 << 18
 
@@ -202,3 +227,49 @@ def hand_table() -> np.ndarray:
     if _TABLE_CACHE is None:
         _TABLE_CACHE = generate_hand_table()
     return _TABLE_CACHE
+
+
+def br_options(threads: int = 0, flop_stride: int = 1, verbose: bool = False, iso_check: bool = False) -> BrOptions:
+    o = BrOptions()
+    o.threads = int(threads)
+    o.flop_stride = int(flop_stride)
+    o.flags = (BR_VERBOSE if verbose else 0) | (BR_ISO_CHECK if iso_check else 0)
+    return o
+
+
+def subgame_struct(street: int, pot: int, board, ranges: np.ndarray) -> tuple[Subgame, np.ndarray]:
+    """A Subgame struct and the float32 range array it points to (keep both alive)."""
+    r = np.ascontiguousarray(ranges, dtype=np.float32)
+    sg = Subgame()
+    sg.street = int(street)
+    sg.pot = int(pot)
+    for i, c in enumerate(list(board)[:5]):
+        sg.board[i] = int(c)
+    sg.ranges = r.ctypes.data
+    return sg, r
+
+
+def best_response(config: Config, hand_table_: np.ndarray, keys: np.ndarray, strategy_sum: np.ndarray,
+                  subgame: dict | None = None, **opts) -> dict:
+    """Heads-up best response of rows (keys, strategy_sum [n][8]) on the host
+    (mccfr_best_response); subgame = dict(street, pot, board, ranges) or None
+    for the full game."""
+    lib = load()
+    t = np.ascontiguousarray(hand_table_, dtype=np.int32)
+    k = np.ascontiguousarray(keys, dtype=np.uint64)
+    s = np.ascontiguousarray(strategy_sum, dtype=np.float32).reshape(-1, 8)
+    sgp = None
+    if subgame is not None:
+        sg, _keep = subgame_struct(subgame["street"], subgame["pot"], subgame["board"], subgame["ranges"])
+        sgp = ctypes.byref(sg)
+    out = Exploit()
+    check(lib.mccfr_best_response(ctypes.byref(config), sgp, ptr(t), t.size, ptr(k), ptr(s), k.size,
+                                  ctypes.byref(br_options(**opts)), ctypes.byref(out)))
+    return out.as_dict()
+
+
+def rank_cdf_lut(hand_table_: np.ndarray, ncards: int, buckets: int) -> np.ndarray:
+    t = np.ascontiguousarray(hand_table_, dtype=np.int32)
+    out = np.zeros(7463, dtype=np.uint8)
+    check(load().mccfr_rank_cdf_lut(ptr(t), t.size, int(ncards), int(buckets), ptr(out)))
+    return out

@@ -57,13 +57,8 @@ class GPUCFRTrainer:
         self = cls.__new__(cls)
         self._lib = L.load()
         self.config = config
-        r = np.ascontiguousarray(ranges, dtype=np.float32).reshape(config.num_players, 1326)
-        sg = L.Subgame()
-        sg.street = int(street)
-        sg.pot = int(pot)
-        for i, c in enumerate(list(board)[:5]):
-            sg.board[i] = int(c)
-        sg.ranges = r.ctypes.data
+        sg, _keep = L.subgame_struct(street, pot, board,
+                                     np.asarray(ranges, dtype=np.float32).reshape(config.num_players, 1326))
         h = c_void_p()
         L.check(self._lib.mccfr_create_subgame(byref(config), byref(sg), byref(h)))
         self._h = h
@@ -188,6 +183,15 @@ class GPUCFRTrainer:
         p = c_void_p()
         L.check(self._lib.mccfr_get_stream(self._h, byref(p)), self._h)
         return int(p.value or 0)
+
+    def exploitability(self, threads: int = 0, flop_stride: int = 1, verbose: bool = False,
+                       iso_check: bool = False) -> dict:
+        """Heads-up best response to the current average strategy, FP64 on host
+        threads (mccfr_exploitability)."""
+        out = L.Exploit()
+        opts = L.br_options(threads, flop_stride, verbose, iso_check)
+        L.check(self._lib.mccfr_exploitability(self._h, byref(opts), byref(out)), self._h)
+        return out.as_dict()
 
     def eval7(self, cards: np.ndarray) -> np.ndarray:
         c = np.ascontiguousarray(cards, dtype=np.uint8).reshape(-1, 7)
