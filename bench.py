@@ -36,6 +36,7 @@ WORKLOADS = {
     "6max-100bb": ("PRESET_6MAX_100BB", {}, 1 << 20),
     "6max-100bb-refrule": ("PRESET_6MAX_100BB", {"sampling": 0, "max_depth": 64}, 1 << 20),
     "hu-20bb": ("PRESET_HU_20BB", {}, 1 << 16),
+    "hu-20bb-refrule": ("PRESET_HU_20BB", {"sampling": 0}, 1 << 16),
     "ref8-6max": ("PRESET_REF8", {"num_players": 6, "table_log2": 27}, 1 << 18),
     "ref8-hu": ("PRESET_REF8", {"table_log2": 27}, 1 << 16),
 }
@@ -53,6 +54,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--table-log2", type=int, default=0, help="override the table capacity (profiling cases)")
     ap.add_argument("--key-bits", type=int, default=-1, help="override the hashed key width (profiling cases)")
+    ap.add_argument("--hu-exploitability", type=int, default=0, metavar="ITERS",
+                    help="only: train heads-up 20BB for ITERS iterations with each update rule and print the "
+                         "exact best-response exploitability of both (a long run; one JSON line)")
+    ap.add_argument("--br-flop-stride", type=int, default=1, help="with --hu-exploitability: flop-class stride")
     return ap.parse_args()
 
 
@@ -297,6 +302,73 @@ def serving_sweep(m, L, table, rates=(10, 30, 100, 300, 1000), n_requests=48) ->
     return out
 
 
+def hu_subgame_exploitability(m, L, table, checkpoints=(10, 40, 160, 640), batch=2048) -> dict:
+    """Exact FP64 best response of a heads-up river re-solve trained on the GPU
+    by each update rule, at equal iterations (mccfr_exploitability)."""
+    import numpy as np
+
+    rng = np.random.default_rng(12)
+    board = [int(c) for c in rng.permutation(52)[:5]]
+    cards = np.array([(lo, hi) for hi in range(1, 52) for lo in range(hi)])
+    blocked = np.isin(cards, board).any(axis=1)
+    ranges = np.zeros((2, 1326))
+    for p in range(2):
+        idx = rng.permutation(np.flatnonzero(~blocked))[:200]
+        ranges[p, idx] = rng.dirichlet(np.full(200, 1.0))
+    ranges = ranges.astype(np.float32)
+    owner = m.GPUCFRTrainer(config=L.preset(L.PRESET_HU_20BB), table_log2=10)
+    owner.set_hand_table(table)
+    out = {}
+    for name, sampling in (("external", L.SAMPLING_EXTERNAL), ("reference_rule", L.SAMPLING_REFERENCE)):
+        c = L.preset(L.PRESET_HU_20BB)
+        c.starting_stack = 10000
+        slots = [(L.ACT_FOLD, 0, 1), (L.ACT_CHECK_CALL, 0, 1), (L.ACT_RAISE_POT, 1, 2), (L.ACT_RAISE_POT, 1, 1),
+                 (L.ACT_ALL_IN, 0, 1)]
+        c.num_actions = len(slots)
+        for a, (k, n, d) in enumerate(slots):
+            c.action_kind[a], c.action_num[a], c.action_den[a] = k, n, d
+        c.raise_cap, c.max_depth, c.table_log2, c.key_bits, c.sampling = 2, 255, 18, 17, sampling
+        tr = m.GPUCFRTrainer.subgame(c, 3, 1200, board, ranges)
+        tr.share_hand_table(owner)
+        done, curve = 0, []
+        for k in checkpoints:
+            tr.train(k - done, batch, verbose=False)
+            done = k
+            e = tr.exploitability()
+            curve.append({"iterations": k, "mbb_per_game": e["mbb_per_game"], "br_seconds": round(e["seconds"], 3)})
+        out[name] = curve
+        tr.close()
+    owner.close()
+    out["workload"] = (f"heads-up river subgame, 100BB stacks, pot 12BB, 200-combo Dirichlet(1) ranges (seed 12), "
+                       f"{{fold, check/call, 1/2 pot, pot, all-in}}, raise cap 2, {batch} traversals per update; "
+                       "exact FP64 best response (mccfr_exploitability)")
+    return out
+
+
+def hu_full_exploitability(m, L, table, iters: int, stride: int) -> dict:
+    """Heads-up 20BB from the blinds: both update rules trained for `iters`
+    iterations of 65,536 traversals per player-update, then the exact best
+    response of each average strategy (all 1,755 flop classes unless a stride
+    is given)."""
+    out = {"iterations": iters, "traversals_per_update": 1 << 16, "flop_stride": stride}
+    for wl in ("hu-20bb", "hu-20bb-refrule"):
+        cfg, batch = make_config(L, wl)
+        tr = m.GPUCFRTrainer(config=cfg)
+        tr.set_hand_table(table)
+        t0 = time.perf_counter()
+        tr.train(iters, batch, verbose=False)
+        st = tr.stats()
+        train_s = time.perf_counter() - t0
+        e = tr.exploitability(flop_stride=stride, verbose=True)
+        out[wl] = {"train_seconds": train_s, "traversals": st.traversals, "rows_used": st.rows_used,
+                   "traversals_per_s": st.traversals / train_s, **e}
+        tr.close()
+        print(json.dumps({wl: out[wl]}), file=sys.stderr, flush=True)
+    a, b = out["hu-20bb"]["mbb_per_game"], out["hu-20bb-refrule"]["mbb_per_game"]
+    out["external_over_reference_rule"] = a / b
+    return out
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -353,6 +425,11 @@ def main():
         dist.init_process_group(backend, timeout=timedelta(seconds=300))
     cfg.device = local_rank
     table = L.hand_table()
+    if args.hu_exploitability:
+        if rank == 0:
+            print(json.dumps(hu_full_exploitability(m, L, table, args.hu_exploitability, args.br_flop_stride)),
+                  flush=True)
+        return
     tr = m.GPUCFRTrainer(config=cfg)
     tr.set_hand_table(table)
 
@@ -438,6 +515,7 @@ def main():
         extras["batched_same_table"] = batched_same_table(m, L, table, args, value)
         extras["c3_multitable"] = multitable(m, L, table)
         extras["resolve_serving"] = serving_sweep(m, L, table)
+        extras["hu_subgame_exploitability"] = hu_subgame_exploitability(m, L, table)
         for wl in ("ref8-6max", "6max-100bb-refrule"):
             if wl == args.workload:
                 continue

@@ -344,6 +344,30 @@ void node_probs(const RowMap& M, const Node& n, uint64_t key, double* p) {
   }
 }
 
+// ---- suit permutations ------------------------------------------------------
+struct SuitPerms {
+  int perm[24][4];
+  int inv_combo[24][kC];  // combo index of sigma^-1 applied to the combo
+  SuitPerms() {
+    int p[4] = {0, 1, 2, 3}, n = 0;
+    do {
+      for (int i = 0; i < 4; ++i) perm[n][i] = p[i];
+      ++n;
+    } while (std::next_permutation(p, p + 4));
+    const Combos& K = CB();
+    for (int s = 0; s < 24; ++s) {
+      int inv[4];
+      for (int i = 0; i < 4; ++i) inv[perm[s][i]] = i;
+      for (int c = 0; c < kC; ++c) {
+        const int a = inv[K.lo[c] / 13] * 13 + K.lo[c] % 13;
+        const int b = inv[K.hi[c] / 13] * 13 + K.hi[c] % 13;
+        inv_combo[s][c] = K.index[a][b];
+      }
+    }
+  }
+  int apply(int s, int card) const { return perm[s][card / 13] * 13 + card % 13; }
+};
+
 // Board state of a walk before the river: known cards and, in the full game,
 // the dense-table row of each combo for this street.
 struct Ctx {
@@ -388,6 +412,10 @@ struct Worker {
   std::vector<FlopEntry>* entries = nullptr;
   std::vector<int>* entry_of = nullptr;          // node -> entry
   std::vector<std::vector<double>>* entry_val = nullptr;  // [entry*2 + player][combo]
+  // full game: suit permutations fixing the current flop (identity first);
+  // turn cards related by one of them give permuted values
+  const SuitPerms* perms = nullptr;
+  std::vector<int> stab;
   // board caches of the current flop (full game) or the subgame's board
   uint16_t bidx_flop[kC];
   std::vector<uint16_t> bidx_turn;  // [52][kC]
@@ -713,6 +741,28 @@ void Worker::deal(int next, const Ctx& X, const double* r0, const double* r1, do
     double* c1 = alloc(kC);
     for (int card = 0; card < 52; ++card) {
       if ((X.mask >> card) & 1) continue;
+      // With a suit permutation s fixing the flop, the reaches here are
+      // s-invariant, so the values after turn s(card) are those after `card`
+      // with combos permuted: walk the smallest card of each orbit only.
+      int images[24], orbit = 0;
+      bool rep = true;
+      for (int s : stab) {
+        const int im = perms->apply(s, card);
+        if (im < card) rep = false;
+        bool seen = false;
+        for (int q = 0; q < orbit; ++q) seen |= images[2 * q] == im;
+        if (!seen && orbit < 12) {
+          images[2 * orbit] = im;
+          images[2 * orbit + 1] = s;
+          ++orbit;
+        }
+      }
+      if (!rep) continue;
+      if (orbit == 0) {
+        images[0] = card;
+        images[1] = 0;
+        orbit = 1;
+      }
       Ctx Y;
       turn_ctx(X, card, Y);
       std::memcpy(f0, r0, kC * sizeof(double));
@@ -722,10 +772,20 @@ void Worker::deal(int next, const Ctx& X, const double* r0, const double* r1, do
         f0[c] = 0.0;
         f1[c] = 0.0;
       }
-      walk(next, Y, f0, f1, c0, c1, wch * pw);
-      for (int c = 0; c < kC; ++c) {
-        v0[c] += pw * c0[c];
-        v1[c] += pw * c1[c];
+      walk(next, Y, f0, f1, c0, c1, wch * pw * orbit);
+      for (int q = 0; q < orbit; ++q) {
+        const int* inv = perms->inv_combo[images[2 * q + 1]];
+        if (images[2 * q + 1] == 0) {
+          for (int c = 0; c < kC; ++c) {
+            v0[c] += pw * c0[c];
+            v1[c] += pw * c1[c];
+          }
+        } else {
+          for (int c = 0; c < kC; ++c) {
+            v0[c] += pw * c0[inv[c]];
+            v1[c] += pw * c1[inv[c]];
+          }
+        }
       }
     }
   } else {
@@ -938,30 +998,6 @@ void Worker::rdecision(const Node& n, const RiverBoard& R, const double* r0, con
   top = mark;
 }
 
-// ---- suit permutations ------------------------------------------------------
-struct SuitPerms {
-  int perm[24][4];
-  int inv_combo[24][kC];  // combo index of sigma^-1 applied to the combo
-  SuitPerms() {
-    int p[4] = {0, 1, 2, 3}, n = 0;
-    do {
-      for (int i = 0; i < 4; ++i) perm[n][i] = p[i];
-      ++n;
-    } while (std::next_permutation(p, p + 4));
-    const Combos& K = CB();
-    for (int s = 0; s < 24; ++s) {
-      int inv[4];
-      for (int i = 0; i < 4; ++i) inv[perm[s][i]] = i;
-      for (int c = 0; c < kC; ++c) {
-        const int a = inv[K.lo[c] / 13] * 13 + K.lo[c] % 13;
-        const int b = inv[K.hi[c] / 13] * 13 + K.hi[c] % 13;
-        inv_combo[s][c] = K.index[a][b];
-      }
-    }
-  }
-  int apply(int s, int card) const { return perm[s][card / 13] * 13 + card % 13; }
-};
-
 struct FlopClass {
   uint8_t cards[3];
   std::vector<int> images;  // one permutation per distinct image of the class
@@ -1170,9 +1206,17 @@ int run_best_response(const BrInput& in, const mccfr_br_options& opt, mccfr_expl
           }
         W.walk(E.nodes[F.node].next, X, f0.data(), f1.data(), c0.data(), c1.data(), wprof);
       };
+      W.perms = &P;
       for (int k = tid; k < nsel; k += threads) {
         const FlopClass& FC = classes[(size_t)k * stride];
         W.reset_flop_caches();
+        W.stab.clear();
+        for (int s = 0; s < 24; ++s) {
+          int im[3];
+          for (int i = 0; i < 3; ++i) im[i] = P.apply(s, FC.cards[i]);
+          std::sort(im, im + 3);
+          if (im[0] == FC.cards[0] && im[1] == FC.cards[1] && im[2] == FC.cards[2]) W.stab.push_back(s);
+        }
         const double pf = scale / 17296.0;
         for (size_t e = 0; e < entries.size(); ++e) {
           one_flop(FC.cards, entries[e], 0.5 * pf * (double)FC.images.size());
@@ -1196,7 +1240,10 @@ int run_best_response(const BrInput& in, const mccfr_br_options& opt, mccfr_expl
             const double keep0 = W.prof[0], keep1 = W.prof[1];
             const long long keepb = W.boards;
             W.reset_flop_caches();  // the river cache is keyed by (turn, river) of one flop
+            const std::vector<int> keep_stab = W.stab;
+            W.stab.assign(1, 0);  // every turn card walked: checks the turn symmetry too
             one_flop(img, entries[e], 0.0);
+            W.stab = keep_stab;
             W.reset_flop_caches();
             W.prof[0] = keep0;
             W.prof[1] = keep1;
