@@ -147,7 +147,7 @@ k_traverse_batched(const __grid_constant__ PhaseParams P, const DealRec* __restr
       const uint32_t t = (uint32_t)(g - P.off[j]);
       const Sched* sc = D.sched;
       EsCounts c{0, 0, 0};
-      es_walk<W>(D.G, D.tv, deals[g], t, update_id(sc, D.G.N), sc->player, D.rscale, fr, c);
+      es_walk<W>(D.G, D.tv, deals + g, t, update_id(sc, D.G.N), sc->player, D.rscale, fr, c);
       c_trav++;
       c_vis += c.visits;
       c_upd += c.updates;

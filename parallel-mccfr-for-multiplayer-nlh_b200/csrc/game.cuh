@@ -214,6 +214,24 @@ __device__ __forceinline__ void node_strategy(const float* reg, uint32_t vm, flo
   }
 }
 
+// Per-player fields indexed by a runtime player: selects over the unrolled
+// slots, so that a state held by one thread stays in registers instead of
+// being placed in local memory for dynamic indexing.
+template <class T>
+__device__ __forceinline__ int pget(const T (&a)[kMaxPlayers], int p) {
+  int v = a[0];
+#pragma unroll
+  for (int i = 1; i < kMaxPlayers; ++i)
+    if (p == i) v = a[i];
+  return v;
+}
+template <class T>
+__device__ __forceinline__ void pset(T (&a)[kMaxPlayers], int p, int v) {
+#pragma unroll
+  for (int i = 0; i < kMaxPlayers; ++i)
+    if (p == i) a[i] = (T)v;
+}
+
 // Hole-card combo index of two distinct cards: hi*(hi-1)/2 + lo, 0..1325.
 __device__ __forceinline__ int combo_index(int a, int b) {
   const int lo = min(a, b), hi = max(a, b);

@@ -287,6 +287,7 @@ struct mccfr_handle {
   int round_player = 0;          // next player of round-by-round training
   Sched* h_sched = nullptr;  // pinned
   Counters* d_counters = nullptr;
+  unsigned* d_work = nullptr;  // traversal work counter of the persistent kernel
   // graph of one iteration
   cudaGraphExec_t graph = nullptr;
   int graph_batch = -1;
@@ -472,7 +473,7 @@ int enqueue_update(mccfr_handle* h, int batch, mccfr_trace* d_trace, cudaEvent_t
       k_traverse_ref<kRefBlock, false><<<grid, kRefBlock, 0, h->stream>>>(h->gp, h->tv, h->d_deals, h->d_sched,
                                                                             batch, rscale, h->d_counters, nullptr);
   } else {
-    launch_traverse_es(h->gp, h->tv, h->d_deals, h->d_sched, batch, rscale, h->d_counters, h->stream);
+    launch_traverse_es(h->gp, h->tv, h->d_deals, h->d_sched, batch, rscale, h->d_counters, h->d_work, h->stream);
   }
   CK(cudaGetLastError());
   if (ev3 && record(h, ev3[1], capturing)) return MCCFR_ERR_CUDA;
@@ -621,6 +622,7 @@ void release(mccfr_handle* h) {
   cudaFree(h->d_sched);
   cudaFreeHost(h->h_sched);
   cudaFree(h->d_counters);
+  cudaFree(h->d_work);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -782,6 +784,8 @@ int mccfr_create(const mccfr_config* cfg, mccfr_handle** out) {
   CKC(cudaMallocHost(&h->h_sched, sizeof(Sched)));
   CKC(cudaMalloc(&h->d_counters, sizeof(Counters)));
   CKC(cudaMemset(h->d_counters, 0, sizeof(Counters)));
+  CKC(cudaMalloc(&h->d_work, 256));
+  CKC(cudaMemset(h->d_work, 0, 256));
   // Table rows, the touched list and small counters in one allocation.
   h->cap = 1ull << cfg->table_log2;
   const unsigned long long C = h->cap;

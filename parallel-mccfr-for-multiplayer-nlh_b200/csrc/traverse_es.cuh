@@ -45,7 +45,7 @@ constexpr int kMaxFrames = 24;
 __device__ __forceinline__ void es_apply(const GameParams& G, EsState& s, int player, int a) {
   s.q >>= 4;
   s.nq--;
-  const int pstack = s.stack[player], pbet = s.bet[player];
+  const int pstack = pget(s.stack, player), pbet = pget(s.bet, player);
   const int to_call = s.cb - pbet;
   const int chips = chips_for(G, a, s.pot, pstack, to_call, s.cb, s.lfr);
   s.abits = ((s.abits << 3) | (uint32_t)a) & 0x3FFFFFFFu;
@@ -57,9 +57,9 @@ __device__ __forceinline__ void es_apply(const GameParams& G, EsState& s, int pl
   }
   if (k == 1) return;
   const int nstack = pstack - chips, nbet = pbet + chips;
-  s.stack[player] = (uint16_t)nstack;
-  s.bet[player] = (uint16_t)nbet;
-  s.inv[player] = (uint16_t)(s.inv[player] + chips);
+  pset(s.stack, player, nstack);
+  pset(s.bet, player, nbet);
+  pset(s.inv, player, pget(s.inv, player) + chips);
   s.pot += chips;
   if (nstack == 0) s.allin |= (uint8_t)(1u << player);
   if (nbet > s.cb) {
@@ -95,247 +95,306 @@ struct EsCounts {
   unsigned visits, updates, terminals;
 };
 
-// One external-sampling traversal (deal `D`, traversal index t, update uid of
-// player `up`): the updating player's subtree depth-first, opponents sampled.
-template <int W, class Frames>
-__device__ __forceinline__ void es_walk(const GameParams& G, const TableView& tv, const DealRec& D, uint32_t t,
-                                        uint32_t uid, int up, float rscale, Frames& fr, EsCounts& cnt) {
-  const int N = G.N;
-  const int dealer = D.dealer;
-  uint32_t ctx[kMaxPlayers], rank[kMaxPlayers];
-#pragma unroll
-  for (int p = 0; p < kMaxPlayers; ++p) {
-    ctx[p] = D.ctx[p];
-    rank[p] = D.rank[p];
-  }
+// One external-sampling traversal in progress on one lane: the betting state,
+// the frame-stack depth, and the value being handed back up the frames.
+struct EsLane {
   EsState cur;
+  const DealRec* deal;
+  uint32_t t;
+  int dealer;
+  int sp;
+  float value;
+  bool ret;  // returning `value` to the frames
+};
+
+// Root state of traversal t (deal `D`): blinds and the preflop queue, or a
+// subgame's start (cfr_gpu.cu:954-981).
+__device__ __forceinline__ void es_begin(const GameParams& G, const DealRec* D, uint32_t t, EsLane& L) {
+  const int N = G.N;
+  const int dealer = D->dealer;
+  L.deal = D;
+  L.t = t;
+  L.dealer = dealer;
+  L.sp = 0;
+  L.value = 0.0f;
+  L.ret = false;
   if (G.sub_street) {
     // subgame: the dead pot split equally, everyone with the same stack, first
     // to act after the dealer (the last seat)
     for (int p = 0; p < kMaxPlayers; ++p) {
-      cur.stack[p] = (uint16_t)G.stack;
-      cur.bet[p] = 0;
-      cur.inv[p] = (uint16_t)((p < N) ? G.sub_pot / N : 0);
+      L.cur.stack[p] = (uint16_t)G.stack;
+      L.cur.bet[p] = 0;
+      L.cur.inv[p] = (uint16_t)((p < N) ? G.sub_pot / N : 0);
     }
-    cur.pot = G.sub_pot;
-    cur.cb = 0;
-    cur.lfr = G.bb;
-    cur.folded = 0;
-    cur.allin = 0;
-    cur.street = (uint8_t)G.sub_street;
-    cur.raises = 0;
-    cur.abits = 0;
-    cur.path = kPathSeed;
-    cur.depth = 0;
-    cur.q = 0;
-    cur.nq = 0;
-    for (int i = 1; i <= N; ++i) cur.q |= (uint32_t)((dealer + i) % N) << (4 * cur.nq++);
+    L.cur.pot = G.sub_pot;
+    L.cur.cb = 0;
+    L.cur.lfr = G.bb;
+    L.cur.folded = 0;
+    L.cur.allin = 0;
+    L.cur.street = (uint8_t)G.sub_street;
+    L.cur.raises = 0;
+    L.cur.abits = 0;
+    L.cur.path = kPathSeed;
+    L.cur.depth = 0;
+    L.cur.q = 0;
+    L.cur.nq = 0;
+    for (int i = 1; i <= N; ++i) L.cur.q |= (uint32_t)((dealer + i) % N) << (4 * L.cur.nq++);
   } else {
     for (int p = 0; p < kMaxPlayers; ++p) {
-      cur.stack[p] = (uint16_t)G.stack;
-      cur.bet[p] = 0;
-      cur.inv[p] = 0;
+      L.cur.stack[p] = (uint16_t)G.stack;
+      L.cur.bet[p] = 0;
+      L.cur.inv[p] = 0;
     }
     const int sbp = (N == 2) ? dealer : (dealer + 1) % N;
     const int bbp = (N == 2) ? (dealer + 1) % N : (dealer + 2) % N;
     const int sba = min(G.sb, G.stack), bba = min(G.bb, G.stack);
-    cur.stack[sbp] = (uint16_t)(G.stack - sba);
-    cur.bet[sbp] = (uint16_t)sba;
-    cur.inv[sbp] = (uint16_t)sba;
-    cur.stack[bbp] = (uint16_t)(G.stack - bba);
-    cur.bet[bbp] = (uint16_t)bba;
-    cur.inv[bbp] = (uint16_t)bba;
-    cur.pot = sba + bba;
-    cur.cb = bba;
-    cur.lfr = G.bb;
-    cur.folded = 0;
-    cur.allin = 0;
-    if (G.stack - sba == 0) cur.allin |= (uint8_t)(1u << sbp);
-    if (G.stack - bba == 0) cur.allin |= (uint8_t)(1u << bbp);
-    cur.street = 0;
-    cur.raises = 0;
-    cur.abits = 0;
-    cur.path = kPathSeed;
-    cur.depth = 0;
-    cur.q = 0;
-    cur.nq = 0;
+    pset(L.cur.stack, sbp, G.stack - sba);
+    pset(L.cur.bet, sbp, sba);
+    pset(L.cur.inv, sbp, sba);
+    pset(L.cur.stack, bbp, G.stack - bba);
+    pset(L.cur.bet, bbp, bba);
+    pset(L.cur.inv, bbp, bba);
+    L.cur.pot = sba + bba;
+    L.cur.cb = bba;
+    L.cur.lfr = G.bb;
+    L.cur.folded = 0;
+    L.cur.allin = 0;
+    if (G.stack - sba == 0) L.cur.allin |= (uint8_t)(1u << sbp);
+    if (G.stack - bba == 0) L.cur.allin |= (uint8_t)(1u << bbp);
+    L.cur.street = 0;
+    L.cur.raises = 0;
+    L.cur.abits = 0;
+    L.cur.path = kPathSeed;
+    L.cur.depth = 0;
+    L.cur.q = 0;
+    L.cur.nq = 0;
     for (int i = 0; i < N; ++i) {
       const int p = (bbp + 1 + i) % N;
-      if (!((cur.allin >> p) & 1)) cur.q |= (uint32_t)p << (4 * cur.nq++);
+      if (!((L.cur.allin >> p) & 1)) L.cur.q |= (uint32_t)p << (4 * L.cur.nq++);
     }
   }
 
-  int sp = 0;
-  unsigned n_visits = 0, n_updates = 0, n_term = 0;
-  const uint32_t all_players = (1u << N) - 1;
-  bool aborted = false;
-
-  for (;;) {
-    // ---- descend from `cur` to a terminal value or an updating-player node
-    float value = 0.0f;
-    bool pushed = false;
-    for (;;) {
-      if (cur.depth >= G.max_depth) {
-        value = 0.0f;
-        n_term++;
-        break;
-      }
-      const uint32_t live = all_players & ~(uint32_t)cur.folded;
-      if (__popc(live) == 1) {
-        const int winner = __ffs(live) - 1;
-        value = (winner == up) ? (float)(cur.pot - (int)cur.inv[up]) : (float)(-(int)cur.inv[up]);
-        n_term++;
-        break;
-      }
-      if (cur.nq == 0) {
-        if (cur.street < 3) {
-          cur.street++;
-          for (int p = 0; p < kMaxPlayers; ++p) cur.bet[p] = 0;
-          cur.cb = 0;
-          cur.lfr = G.bb;
-          cur.raises = 0;
-          cur.q = 0;
-          cur.nq = 0;
-          for (int i = 1; i <= N; ++i) {
-            const int p = (dealer + i) % N;
-            if (!((cur.folded >> p) & 1) && !((cur.allin >> p) & 1)) cur.q |= (uint32_t)p << (4 * cur.nq++);
-          }
-          if (cur.nq > 0) {
-            cur.depth++;
-            continue;
-          }
-        }
-        value = side_pot_payoff(
-            N, up, cur.folded, [&](int q) { return (int)cur.inv[q]; }, [&](int q) { return rank[q]; });
-        n_term++;
-        break;
-      }
-      const int player = (int)(cur.q & 0xF);
-      const int to_call = cur.cb - (int)cur.bet[player];
-      const uint32_t vm = valid_mask(G, cur.pot, cur.stack[player], to_call, cur.cb, cur.lfr, cur.raises);
-      const uint32_t cw = ctx[player];
-      uint32_t hb, bkt;
-      if (G.sub_street) {  // exact combo; the river card once it is dealt
-        hb = cw & 0xFFFF;
-        bkt = (cur.street == 3 && G.sub_street == 2) ? (cw >> 16) : 0u;
-      } else {
-        hb = cw & 0xFF;
-        bkt = cur.street ? ((cw >> (8 * cur.street)) & 0xFF) : 0u;
-      }
-      const unsigned long long key = info_key(G, player, hb, bkt, cur.street, cur.abits, cur.path);
-      const long long slot = table_insert<W>(tv, key);
-      float reg[kSlots];
-      load_regrets(tv, slot, reg);
-      n_visits++;
-      if (player == up) {
-        if (sp >= kMaxFrames || slot < 0) {
-          if (sp >= kMaxFrames) atomicOr(tv.err, kErrStackOverflow);
-          aborted = true;
-          break;
-        }
-        EsFrame& F = fr.at(sp++);
-        F.st = cur;
-        node_strategy(reg, vm, F.strat);
-        F.vh = 0.0f;
-        F.slot = (uint32_t)slot;
-        F.vm = (uint8_t)vm;
-        F.player = (uint8_t)player;
-        const int a0 = __ffs(vm) - 1;
-        F.next_a = (uint8_t)a0;
-        es_apply(G, cur, player, a0);
-        cur.depth++;
-        pushed = true;
-        continue;
-      }
-      // sampled opponent: strategy sum, then one action
-      const U4 d = philox(U4{t, uid, (uint32_t)cur.path, (uint32_t)(cur.path >> 32) | 0x80000000u},
-                          G.seed_lo, G.seed_hi);
-      const int s = sample_action(G, reg, vm, uniform01(d.x));
-      if (slot >= 0) {
-        if (touch_row(tv, (unsigned long long)slot, uid, vm)) {
-          atomicAdd(row_cnt(tv, slot), (1ull << 32) | 1ull);
-        } else {
-          atomicAdd(row_cnt(tv, slot), 1ull << 32);
-          float strat[kSlots];
-          node_strategy(reg, vm, strat);
-          long long dw[kSlots];
-#pragma unroll
-          for (int a = 0; a < kSlots; ++a) dw[a] = fix_s(strat[a]);
-          add_direct(tv, slot, vm, nullptr, dw);
-        }
-      }
-      es_apply(G, cur, player, s);
-      cur.depth++;
-    }
-    (void)pushed;
-    if (aborted) break;
-    // ---- return `value` to the frames
-    bool resumed = false;
-    while (sp > 0) {
-      EsFrame& F = fr.at(sp - 1);
-      const int a = F.next_a;
-      atomicAdd(row_da(tv, F.slot) + a, (unsigned long long)fix_r(value, rscale));
-      F.vh = __fadd_rn(F.vh, __fmul_rn(F.strat[a], value));
-      const uint32_t rest = (uint32_t)F.vm & ~((2u << a) - 1u);
-      if (rest) {
-        const int nx = __ffs(rest) - 1;
-        F.next_a = (uint8_t)nx;
-        cur = F.st;
-        es_apply(G, cur, F.player, nx);
-        cur.depth++;
-        resumed = true;
-        break;
-      }
-      // node complete
-      const float vh = F.vh;
-      const long long fv = fix_r(vh, rscale);
-      atomicAdd(row_cnt(tv, F.slot), 1ull << 32);
-      if (touch_row(tv, F.slot, uid, F.vm)) {
-        atomicAdd(row_su(tv, F.slot), (unsigned long long)fv);
-      } else {
-        long long dr[kSlots];
-#pragma unroll
-        for (int b = 0; b < kSlots; ++b) dr[b] = -fv;
-        add_direct(tv, F.slot, F.vm, dr, nullptr);
-      }
-      n_updates++;
-      value = vh;
-      sp--;
-    }
-    if (!resumed) break;
-  }
-  cnt.visits += n_visits;
-  cnt.updates += n_updates;
-  cnt.terminals += n_term;
 }
 
+// One event of a traversal: a descend step (one decision node, a street change
+// or a terminal) or a return step (one child value handed to the top frame).
+// Returns 0 while the traversal goes on, 1 when it is complete, 2 when it
+// stopped on a full table or frame stack (the error flag is set).  The updating
+// player's subtree is walked depth-first, opponents sampled.
+template <int W, class Frames>
+__device__ __forceinline__ int es_step(const GameParams& G, const TableView& tv, uint32_t uid, int up, float rscale,
+                                       Frames& fr, EsLane& L, EsCounts& cnt) {
+  const int N = G.N;
+  const uint32_t all_players = (1u << N) - 1;
+  EsState& cur = L.cur;
+  const uint32_t t = L.t;
+  if (!L.ret) {
+    if (cur.depth >= G.max_depth) {
+      L.value = 0.0f;
+      cnt.terminals++;
+      L.ret = true;
+      return 0;
+    }
+    const uint32_t live = all_players & ~(uint32_t)cur.folded;
+    if (__popc(live) == 1) {
+      const int winner = __ffs(live) - 1;
+      const int inv_up = pget(cur.inv, up);
+      L.value = (winner == up) ? (float)(cur.pot - inv_up) : (float)(-inv_up);
+      cnt.terminals++;
+      L.ret = true;
+      return 0;
+    }
+    if (cur.nq == 0) {
+      if (cur.street < 3) {
+        cur.street++;
+        for (int p = 0; p < kMaxPlayers; ++p) cur.bet[p] = 0;
+        cur.cb = 0;
+        cur.lfr = G.bb;
+        cur.raises = 0;
+        cur.q = 0;
+        cur.nq = 0;
+        for (int i = 1; i <= N; ++i) {
+          const int p = (L.dealer + i) % N;
+          if (!((cur.folded >> p) & 1) && !((cur.allin >> p) & 1)) cur.q |= (uint32_t)p << (4 * cur.nq++);
+        }
+        if (cur.nq > 0) {
+          cur.depth++;
+          return 0;
+        }
+      }
+      const DealRec* D = L.deal;
+      L.value = side_pot_payoff(
+          N, up, cur.folded, [&](int q) { return pget(cur.inv, q); }, [&](int q) { return (uint32_t)__ldg(D->rank + q); });
+      cnt.terminals++;
+      L.ret = true;
+      return 0;
+    }
+    const int player = (int)(cur.q & 0xF);
+    const int to_call = cur.cb - pget(cur.bet, player);
+    const uint32_t vm = valid_mask(G, cur.pot, pget(cur.stack, player), to_call, cur.cb, cur.lfr, cur.raises);
+    const uint32_t cw = __ldg(L.deal->ctx + player);
+    uint32_t hb, bkt;
+    if (G.sub_street) {  // exact combo; the river card once it is dealt
+      hb = cw & 0xFFFF;
+      bkt = (cur.street == 3 && G.sub_street == 2) ? (cw >> 16) : 0u;
+    } else {
+      hb = cw & 0xFF;
+      bkt = cur.street ? ((cw >> (8 * cur.street)) & 0xFF) : 0u;
+    }
+    const unsigned long long key = info_key(G, player, hb, bkt, cur.street, cur.abits, cur.path);
+    const long long slot = table_insert<W>(tv, key);
+    float reg[kSlots];
+    load_regrets(tv, slot, reg);
+    cnt.visits++;
+    if (player == up) {
+      if (L.sp >= kMaxFrames || slot < 0) {
+        if (L.sp >= kMaxFrames) atomicOr(tv.err, kErrStackOverflow);
+        return 2;
+      }
+      EsFrame& F = fr.at(L.sp++);
+      F.st = cur;
+      node_strategy(reg, vm, F.strat);
+      F.vh = 0.0f;
+      F.slot = (uint32_t)slot;
+      F.vm = (uint8_t)vm;
+      F.player = (uint8_t)player;
+      const int a0 = __ffs(vm) - 1;
+      F.next_a = (uint8_t)a0;
+      es_apply(G, cur, player, a0);
+      cur.depth++;
+      return 0;
+    }
+    // sampled opponent: strategy sum, then one action
+    const U4 d = philox(U4{t, uid, (uint32_t)cur.path, (uint32_t)(cur.path >> 32) | 0x80000000u},
+                        G.seed_lo, G.seed_hi);
+    const int s = sample_action(G, reg, vm, uniform01(d.x));
+    if (slot >= 0) {
+      if (touch_row(tv, (unsigned long long)slot, uid, vm)) {
+        atomicAdd(row_cnt(tv, slot), (1ull << 32) | 1ull);
+      } else {
+        atomicAdd(row_cnt(tv, slot), 1ull << 32);
+        float strat[kSlots];
+        node_strategy(reg, vm, strat);
+        long long dw[kSlots];
+#pragma unroll
+        for (int a = 0; a < kSlots; ++a) dw[a] = fix_s(strat[a]);
+        add_direct(tv, slot, vm, nullptr, dw);
+      }
+    }
+    es_apply(G, cur, player, s);
+    cur.depth++;
+    return 0;
+  }
+  // ---- return step: `value` to the top frame
+  if (L.sp == 0) return 1;
+  EsFrame& F = fr.at(L.sp - 1);
+  const int a = F.next_a;
+  const float value = L.value;
+  atomicAdd(row_da(tv, F.slot) + a, (unsigned long long)fix_r(value, rscale));
+  F.vh = __fadd_rn(F.vh, __fmul_rn(F.strat[a], value));
+  const uint32_t rest = (uint32_t)F.vm & ~((2u << a) - 1u);
+  if (rest) {
+    const int nx = __ffs(rest) - 1;
+    F.next_a = (uint8_t)nx;
+    cur = F.st;
+    es_apply(G, cur, F.player, nx);
+    cur.depth++;
+    L.ret = false;
+    return 0;
+  }
+  // node complete
+  const float vh = F.vh;
+  const long long fv = fix_r(vh, rscale);
+  atomicAdd(row_cnt(tv, F.slot), 1ull << 32);
+  if (touch_row(tv, F.slot, uid, F.vm)) {
+    atomicAdd(row_su(tv, F.slot), (unsigned long long)fv);
+  } else {
+    long long dr[kSlots];
+#pragma unroll
+    for (int b = 0; b < kSlots; ++b) dr[b] = -fv;
+    add_direct(tv, F.slot, F.vm, dr, nullptr);
+  }
+  cnt.updates++;
+  L.value = vh;
+  L.sp--;
+  return 0;
+}
+
+// One whole traversal (the batched kernel's unit of work).
+template <int W, class Frames>
+__device__ __forceinline__ void es_walk(const GameParams& G, const TableView& tv, const DealRec* D, uint32_t t,
+                                        uint32_t uid, int up, float rscale, Frames& fr, EsCounts& cnt) {
+  EsLane L;
+  es_begin(G, D, t, L);
+  while (es_step<W>(G, tv, uid, up, rscale, fr, L, cnt) == 0) {
+  }
+}
+
+// Persistent traversal kernel: every lane takes its next traversal from the
+// device work counter as soon as its current one is complete (lanes that need
+// work together share one atomic), inside the same one-event-per-iteration
+// loop.  Tree sizes are heavy-tailed, so with one traversal per thread a warp
+// would run as long as its largest tree while the other lanes idle.
 template <int BLOCK, int K, int W>
 __global__ void __launch_bounds__(BLOCK)
 k_traverse_es(const GameParams G, const TableView tv, const DealRec* __restrict__ deals, const Sched* __restrict__ sched,
-              int batch, float rscale, Counters* __restrict__ counters) {
+              int batch, float rscale, Counters* __restrict__ counters, unsigned* __restrict__ work) {
   extern __shared__ EsFrame s_frames[];  // [K][BLOCK]
-  const uint32_t t = blockIdx.x * BLOCK + threadIdx.x;
-  if (t >= (uint32_t)batch) return;
   const int up = sched->player;
   const uint32_t uid = update_id(sched, G.N);
   FrameStack<K> fr;
   fr.smem = s_frames + threadIdx.x;
   fr.stride = BLOCK;
   EsCounts c{0, 0, 0};
-  es_walk<W>(G, tv, deals[t], t, uid, up, rscale, fr, c);
-  warp_add_counters(counters, 1u, c.visits, c.updates, c.terminals, (unsigned)G.N);
+  unsigned trav = 0;
+  const int lane = threadIdx.x & 31;
+  EsLane L;
+  bool have = false, more = true;
+  // The whole warp stays in the loop until every lane is out of work, and
+  // reconverges before each event.
+  for (;;) {
+    __syncwarp();
+    const bool need = !have && more;
+    const unsigned needm = __ballot_sync(0xFFFFFFFFu, need);
+    if (needm) {
+      const int leader = __ffs(needm) - 1;
+      unsigned base = 0;
+      if (lane == leader) base = atomicAdd(work, (unsigned)__popc(needm));
+      base = __shfl_sync(0xFFFFFFFFu, base, leader);
+      if (need) {
+        const uint32_t t = base + (uint32_t)__popc(needm & ((1u << lane) - 1u));
+        if (t < (uint32_t)batch) {
+          es_begin(G, deals + t, t, L);
+          have = true;
+          trav++;
+        } else {
+          more = false;
+        }
+      }
+    }
+    if (!__any_sync(0xFFFFFFFFu, have)) break;
+    if (have && es_step<W>(G, tv, uid, up, rscale, fr, L, c)) have = false;
+  }
+  warp_add_counters(counters, trav, c.visits, c.updates, c.terminals, trav * (unsigned)G.N);
 }
 
+// `work` must be zero when the launch starts; the launch enqueues that reset.
 inline void launch_traverse_es(const GameParams& G, const TableView& tv, const DealRec* deals, const Sched* sched,
-                               int batch, float rscale, Counters* counters, cudaStream_t stream) {
+                               int batch, float rscale, Counters* counters, unsigned* work, cudaStream_t stream) {
   constexpr int B = 128;
-  const int grid = (batch + B - 1) / B;
-  static bool carveout_set = false;  // the walk keeps no shared memory: all of it to L1
-  if (!carveout_set) {
+  static int resident = 0;  // blocks per SM at this kernel's register use
+  if (!resident) {
+    // the walk keeps no shared memory: all of it to L1
     cudaFuncSetAttribute(k_traverse_es<B, 0, 1>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-    carveout_set = true;
+    int per_sm = 0, dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_traverse_es<B, 0, 1>, B, 0);
+    resident = std::max(1, per_sm) * std::max(1, sms);
   }
-  k_traverse_es<B, 0, 1><<<grid, B, 0, stream>>>(G, tv, deals, sched, batch, rscale, counters);
+  const int grid = std::max(1, std::min(resident, (batch + B - 1) / B));
+  cudaMemsetAsync(work, 0, sizeof(unsigned), stream);
+  k_traverse_es<B, 0, 1><<<grid, B, 0, stream>>>(G, tv, deals, sched, batch, rscale, counters, work);
 }
 
 }  // namespace mccfr
