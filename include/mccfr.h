@@ -249,8 +249,9 @@ typedef struct mccfr_batch_tuning {
   int32_t grab;           /* traversals each lane takes per work-queue grab: 1, 2, 4, 8 */
   int32_t smem_frames;    /* frames of each walk's stack staged in shared memory: 0, 2, 4 */
   int32_t probe_width;    /* table keys loaded per probe step: 1 or 2 */
-  int32_t warp_sync;      /* 1: a warp takes 32 traversals at once and starts them together;
-                             0: each lane takes its next traversal as soon as it is idle */
+  int32_t warp_sync;      /* lanes that refill together share one grab of lanes x grab
+                             traversals; 1: interleaved (neighbouring lanes take neighbouring
+                             traversals), 0: each lane a contiguous run of `grab` */
   int32_t reserved[3];
 } mccfr_batch_tuning;
 typedef struct mccfr_batch_stats {

@@ -90,12 +90,16 @@ __device__ __forceinline__ int param_table_of(const PhaseParams& P, unsigned lon
   return lo;
 }
 
-// Persistent external-sampling traversal over a phase's items.  Each lane takes
-// its next `grab` consecutive items from `work` as soon as it is idle (lanes
-// that become idle together share one atomic), so no lane waits for the rest of
-// its warp.  Counters are summed per lane while it stays on one table.
+// Persistent external-sampling traversal over a phase's items, in the plain
+// kernel's lockstep form: every lane handles one event of its current
+// traversal per iteration and the warp reconverges before each event.  A lane
+// that finishes a traversal takes its next item from its current run; lanes
+// whose runs are used up refill together with one atomic on `work` (lanes x
+// grab items, interleaved across the lanes when warp_sync is set, contiguous
+// runs of `grab` otherwise).  Counters are summed per lane while it stays on
+// one table.
 template <int BLOCK, int K, int W>
-__global__ void __launch_bounds__(BLOCK, 2048 / BLOCK / 2)
+__global__ void __launch_bounds__(BLOCK)
 k_traverse_batched(const __grid_constant__ PhaseParams P, const DealRec* __restrict__ deals,
                    unsigned long long* __restrict__ work, int grab, int warp_sync) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -104,56 +108,71 @@ k_traverse_batched(const __grid_constant__ PhaseParams P, const DealRec* __restr
   FrameStack<K> fr;
   fr.smem = s_frames + threadIdx.x;
   fr.stride = BLOCK;
-  int cur_j = -1;
-  unsigned long long c_trav = 0, c_vis = 0, c_upd = 0, c_term = 0;
+  const int lane = threadIdx.x & 31;
+  int cur_j = -1, up = 0;
+  uint32_t uid = 0;
+  unsigned long long c_trav = 0;
+  EsCounts c{0, 0, 0};
   auto flush = [&]() {
     if (cur_j >= 0 && c_trav) {
       Counters* cn = P.T[cur_j].counters;
       atomicAdd(&cn->traversals, c_trav);
-      atomicAdd(&cn->visits, c_vis);
-      atomicAdd(&cn->updates, c_upd);
-      atomicAdd(&cn->terminals, c_term);
+      atomicAdd(&cn->visits, (unsigned long long)c.visits);
+      atomicAdd(&cn->updates, (unsigned long long)c.updates);
+      atomicAdd(&cn->terminals, (unsigned long long)c.terminals);
       atomicAdd(&cn->evals, c_trav * (unsigned long long)P.T[cur_j].G.N);
     }
-    c_trav = c_vis = c_upd = c_term = 0;
+    c_trav = 0;
+    c = EsCounts{0, 0, 0};
   };
-  const int lane = threadIdx.x & 31;
+  unsigned long long nxt = 0, stop = 0, step = 1;  // this lane's run: nxt, nxt + step, ... < stop
+  bool have = false, more = true;
+  EsLane L;
   for (;;) {
-    unsigned long long base = 0, stride = 1;
-    if (warp_sync) {
-      // the whole warp takes 32*grab items and starts them together
-      if (lane == 0) base = atomicAdd(work, 32ull * grab);
-      base = __shfl_sync(0xFFFFFFFFu, base, 0) + lane;
-      stride = 32;
-      if (base - lane >= total) break;
-    } else {
-      // idle lanes that arrive together take consecutive chunks with one atomic
-      const unsigned act = __activemask();
-      const int leader = __ffs(act) - 1;
-      const int rank = __popc(act & ((1u << lane) - 1));
-      if (lane == leader) base = atomicAdd(work, (unsigned long long)__popc(act) * grab);
-      base = __shfl_sync(act, base, leader) + (unsigned long long)rank * grab;
-      if (base >= total) break;
+    __syncwarp();
+    const bool need = !have && more;
+    const bool refill = need && nxt >= stop;
+    const unsigned rm = __ballot_sync(0xFFFFFFFFu, refill);
+    if (rm) {
+      const int k = __popc(rm);
+      const int leader = __ffs(rm) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(work, (unsigned long long)k * grab);
+      base = __shfl_sync(0xFFFFFFFFu, base, leader);
+      if (refill) {
+        const int r = __popc(rm & ((1u << lane) - 1u));
+        if (warp_sync) {
+          nxt = base + r;
+          step = k;
+          stop = base + (unsigned long long)k * grab;
+        } else {
+          nxt = base + (unsigned long long)r * grab;
+          step = 1;
+          stop = nxt + grab;
+        }
+        if (stop > total) stop = total;
+        if (nxt >= total) more = false;
+      }
     }
-    for (int k = 0; k < grab; ++k) {
-      const unsigned long long g = base + k * stride;
-      if (g >= total) break;
+    if (need && more && nxt < stop) {
+      const unsigned long long g = nxt;
+      nxt += step;
       const int j = param_table_of(P, g);
       if (j != cur_j) {
         flush();
         cur_j = j;
+        uid = update_id(P.T[j].sched, P.T[j].G.N);
+        up = P.T[j].sched->player;
       }
-      const TableDesc& D = P.T[j];
-      const uint32_t t = (uint32_t)(g - P.off[j]);
-      const Sched* sc = D.sched;
-      EsCounts c{0, 0, 0};
-      es_walk<W>(D.G, D.tv, deals + g, t, update_id(sc, D.G.N), sc->player, D.rscale, fr, c);
+      es_begin(P.T[j].G, deals + g, (uint32_t)(g - P.off[j]), L);
+      have = true;
       c_trav++;
-      c_vis += c.visits;
-      c_upd += c.updates;
-      c_term += c.terminals;
     }
-    if (warp_sync) __syncwarp();
+    if (!__any_sync(0xFFFFFFFFu, have || more)) break;
+    if (have) {
+      const TableDesc& D = P.T[cur_j];
+      if (es_step<W>(D.G, D.tv, uid, up, D.rscale, fr, L, c)) have = false;
+    }
   }
   flush();
 }

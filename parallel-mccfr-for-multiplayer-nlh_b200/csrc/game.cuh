@@ -33,6 +33,7 @@ struct GameParams {
   uint8_t n_fallback;
   uint8_t fallback[kSlots];
   uint8_t default_slot;
+  int stack_base;  // chips behind plus chips already in: stack + (subgame) pot share
 };
 
 // ---------------------------------------------------------------------------

@@ -398,6 +398,7 @@ void make_params(const mccfr_config& c, GameParams& g) {
   g.seed_lo = (uint32_t)c.seed;
   g.seed_hi = (uint32_t)(c.seed >> 32);
   g.key_bits = c.key_mode == MCCFR_KEY_ID64 ? c.key_bits : 0;
+  g.stack_base = c.starting_stack;
   for (int a = 0; a < 8; ++a) {
     g.kind[a] = (int8_t)(a < c.num_actions ? c.action_kind[a] : -1);
     g.num[a] = (int16_t)(a < c.num_actions ? c.action_num[a] : 0);
@@ -1678,7 +1679,8 @@ int mccfr_create_subgame(const mccfr_config* cfg, const mccfr_subgame* sg, mccfr
     if (sg->board[i] > 51 || ((mask >> sg->board[i]) & 1)) return MCCFR_ERR_INVALID_ARG;
     mask |= 1ull << sg->board[i];
   }
-  if (sg->pot < 0 || sg->pot % cfg->num_players != 0 || sg->pot / cfg->num_players > 65535)
+  // invested chips are 16-bit: a player's pot share plus its whole stack must fit
+  if (sg->pot < 0 || sg->pot % cfg->num_players != 0 || sg->pot / cfg->num_players + cfg->starting_stack > 65535)
     return MCCFR_ERR_INVALID_ARG;
   std::vector<uint32_t> cdf((size_t)cfg->num_players * 1326);
   for (int p = 0; p < cfg->num_players; ++p)
@@ -1697,6 +1699,7 @@ int mccfr_create_subgame(const mccfr_config* cfg, const mccfr_subgame* sg, mccfr
   }
   h->gp.sub_street = sg->street;
   h->gp.sub_pot = sg->pot;
+  h->gp.stack_base = cfg->starting_stack + sg->pot / cfg->num_players;
   for (int i = 0; i < 5; ++i) h->gp.sub_board[i] = (i < nb) ? sg->board[i] : 0;
   h->gp.range_cdf = h->d_ranges;
   return MCCFR_OK;
@@ -1892,6 +1895,7 @@ int mccfr_best_response(const mccfr_config* cfg, const mccfr_subgame* sg, const 
     if (sg->pot < 0 || sg->pot % 2 != 0) return MCCFR_ERR_INVALID_ARG;
     g.sub_street = sg->street;
     g.sub_pot = sg->pot;
+    g.stack_base = cfg->starting_stack + sg->pot / 2;
     for (int i = 0; i < 5; ++i) g.sub_board[i] = (i < nb) ? sg->board[i] : 0;
     for (int p = 0; p < 2; ++p) {
       uint32_t cdf[1326];

@@ -22,7 +22,9 @@
 namespace mccfr {
 
 struct EsState {
-  uint16_t stack[kMaxPlayers], bet[kMaxPlayers], inv[kMaxPlayers];
+  // chips put in this street and in the hand; a player's stack is
+  // stack_base(G) - inv (es_stack)
+  uint16_t bet[kMaxPlayers], inv[kMaxPlayers];
   int pot;
   int cb, lfr;
   uint32_t q;        // action queue, 4-bit entries
@@ -30,6 +32,12 @@ struct EsState {
   uint64_t path;
   uint8_t folded, allin, street, raises, nq, depth, pad0, pad1;
 };
+
+// Chips behind of `player`: everyone starts with G.stack behind and, in a
+// subgame, an equal share of the dead pot already invested.
+__device__ __forceinline__ int es_stack(const GameParams& G, const EsState& s, int player) {
+  return G.stack_base - pget(s.inv, player);
+}
 
 struct EsFrame {
   EsState st;
@@ -45,7 +53,7 @@ constexpr int kMaxFrames = 24;
 __device__ __forceinline__ void es_apply(const GameParams& G, EsState& s, int player, int a) {
   s.q >>= 4;
   s.nq--;
-  const int pstack = pget(s.stack, player), pbet = pget(s.bet, player);
+  const int pstack = es_stack(G, s, player), pbet = pget(s.bet, player);
   const int to_call = s.cb - pbet;
   const int chips = chips_for(G, a, s.pot, pstack, to_call, s.cb, s.lfr);
   s.abits = ((s.abits << 3) | (uint32_t)a) & 0x3FFFFFFFu;
@@ -57,7 +65,6 @@ __device__ __forceinline__ void es_apply(const GameParams& G, EsState& s, int pl
   }
   if (k == 1) return;
   const int nstack = pstack - chips, nbet = pbet + chips;
-  pset(s.stack, player, nstack);
   pset(s.bet, player, nbet);
   pset(s.inv, player, pget(s.inv, player) + chips);
   s.pot += chips;
@@ -122,7 +129,6 @@ __device__ __forceinline__ void es_begin(const GameParams& G, const DealRec* D, 
     // subgame: the dead pot split equally, everyone with the same stack, first
     // to act after the dealer (the last seat)
     for (int p = 0; p < kMaxPlayers; ++p) {
-      L.cur.stack[p] = (uint16_t)G.stack;
       L.cur.bet[p] = 0;
       L.cur.inv[p] = (uint16_t)((p < N) ? G.sub_pot / N : 0);
     }
@@ -141,17 +147,14 @@ __device__ __forceinline__ void es_begin(const GameParams& G, const DealRec* D, 
     for (int i = 1; i <= N; ++i) L.cur.q |= (uint32_t)((dealer + i) % N) << (4 * L.cur.nq++);
   } else {
     for (int p = 0; p < kMaxPlayers; ++p) {
-      L.cur.stack[p] = (uint16_t)G.stack;
       L.cur.bet[p] = 0;
       L.cur.inv[p] = 0;
     }
     const int sbp = (N == 2) ? dealer : (dealer + 1) % N;
     const int bbp = (N == 2) ? (dealer + 1) % N : (dealer + 2) % N;
     const int sba = min(G.sb, G.stack), bba = min(G.bb, G.stack);
-    pset(L.cur.stack, sbp, G.stack - sba);
     pset(L.cur.bet, sbp, sba);
     pset(L.cur.inv, sbp, sba);
-    pset(L.cur.stack, bbp, G.stack - bba);
     pset(L.cur.bet, bbp, bba);
     pset(L.cur.inv, bbp, bba);
     L.cur.pot = sba + bba;
@@ -231,7 +234,7 @@ __device__ __forceinline__ int es_step(const GameParams& G, const TableView& tv,
     }
     const int player = (int)(cur.q & 0xF);
     const int to_call = cur.cb - pget(cur.bet, player);
-    const uint32_t vm = valid_mask(G, cur.pot, pget(cur.stack, player), to_call, cur.cb, cur.lfr, cur.raises);
+    const uint32_t vm = valid_mask(G, cur.pot, es_stack(G, cur, player), to_call, cur.cb, cur.lfr, cur.raises);
     const uint32_t cw = __ldg(L.deal->ctx + player);
     uint32_t hb, bkt;
     if (G.sub_street) {  // exact combo; the river card once it is dealt

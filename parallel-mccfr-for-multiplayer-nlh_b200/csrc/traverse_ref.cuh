@@ -282,28 +282,46 @@ __global__ void __launch_bounds__(128) k_deal(const GameParams G, const HandView
 // array; invested chips and ranks are read through the caller's accessors.
 template <class InvF, class RankF>
 __device__ __forceinline__ float side_pot_payoff(int N, int up, uint32_t folded, InvF inv, RankF rank) {
-  float payoff = -(float)inv(up);
+  // The players' amounts and ranks are read once into fixed slots, so the
+  // loops below index them with constants.
+  int iv[kMaxPlayers];
+  uint32_t rk[kMaxPlayers];
+#pragma unroll
+  for (int q = 0; q < kMaxPlayers; ++q) {
+    iv[q] = q < N ? inv(q) : 0;
+    rk[q] = q < N ? (uint32_t)rank(q) : 0u;
+  }
+  int inv_up = 0;
+  uint32_t rk_up = 0;
+#pragma unroll
+  for (int q = 0; q < kMaxPlayers; ++q)
+    if (q == up) {
+      inv_up = iv[q];
+      rk_up = rk[q];
+    }
+  const bool up_live = !((folded >> up) & 1);
+  float payoff = -(float)inv_up;
   int prev = 0;
   for (int guard = 0; guard < kMaxPlayers; ++guard) {
     int L = 0x7FFFFFFF;
-    for (int q = 0; q < N; ++q) {
-      const int v = inv(q);
-      if (v > prev && v < L) L = v;
-    }
+#pragma unroll
+    for (int q = 0; q < kMaxPlayers; ++q)
+      if (q < N && iv[q] > prev && iv[q] < L) L = iv[q];
     if (L == 0x7FFFFFFF) break;
     int layer = 0;
     uint32_t best = 0;
-    for (int q = 0; q < N; ++q) {
-      const int v = inv(q);
-      layer += max(0, min(v, L) - prev);
-      if (!((folded >> q) & 1) && v >= L) best = max(best, (uint32_t)rank(q));
-    }
+#pragma unroll
+    for (int q = 0; q < kMaxPlayers; ++q)
+      if (q < N) {
+        layer += max(0, min(iv[q], L) - prev);
+        if (!((folded >> q) & 1) && iv[q] >= L) best = max(best, rk[q]);
+      }
     if (best > 0) {
       int nwin = 0;
-      for (int q = 0; q < N; ++q)
-        if (!((folded >> q) & 1) && inv(q) >= L && (uint32_t)rank(q) == best) nwin++;
-      if (!((folded >> up) & 1) && inv(up) >= L && (uint32_t)rank(up) == best)
-        payoff = __fadd_rn(payoff, __fdiv_rn((float)layer, (float)nwin));
+#pragma unroll
+      for (int q = 0; q < kMaxPlayers; ++q)
+        if (q < N && !((folded >> q) & 1) && iv[q] >= L && rk[q] == best) nwin++;
+      if (up_live && inv_up >= L && rk_up == best) payoff = __fadd_rn(payoff, __fdiv_rn((float)layer, (float)nwin));
     }
     prev = L;
   }
