@@ -191,6 +191,9 @@ __device__ __forceinline__ int es_step(const GameParams& G, const TableView& tv,
   const uint32_t all_players = (1u << N) - 1;
   EsState& cur = L.cur;
   const uint32_t t = L.t;
+  // the action to apply: every branch that moves to a child ends at one
+  // es_apply below, so lanes of a warp in different branches apply together
+  int ap = 0, aa = 0;
   if (!L.ret) {
     if (cur.depth >= G.max_depth) {
       L.value = 0.0f;
@@ -263,63 +266,64 @@ __device__ __forceinline__ int es_step(const GameParams& G, const TableView& tv,
       F.player = (uint8_t)player;
       const int a0 = __ffs(vm) - 1;
       F.next_a = (uint8_t)a0;
-      es_apply(G, cur, player, a0);
-      cur.depth++;
+      ap = player;
+      aa = a0;
+    } else {
+      // sampled opponent: strategy sum, then one action
+      const U4 d = philox(U4{t, uid, (uint32_t)cur.path, (uint32_t)(cur.path >> 32) | 0x80000000u},
+                          G.seed_lo, G.seed_hi);
+      const int s = sample_action(G, reg, vm, uniform01(d.x));
+      if (slot >= 0) {
+        if (touch_row(tv, (unsigned long long)slot, uid, vm)) {
+          atomicAdd(row_cnt(tv, slot), (1ull << 32) | 1ull);
+        } else {
+          atomicAdd(row_cnt(tv, slot), 1ull << 32);
+          float strat[kSlots];
+          node_strategy(reg, vm, strat);
+          long long dw[kSlots];
+#pragma unroll
+          for (int a = 0; a < kSlots; ++a) dw[a] = fix_s(strat[a]);
+          add_direct(tv, slot, vm, nullptr, dw);
+        }
+      }
+      ap = player;
+      aa = s;
+    }
+  } else {
+    // ---- return step: `value` to the top frame
+    if (L.sp == 0) return 1;
+    EsFrame& F = fr.at(L.sp - 1);
+    const int a = F.next_a;
+    const float value = L.value;
+    atomicAdd(row_da(tv, F.slot) + a, (unsigned long long)fix_r(value, rscale));
+    F.vh = __fadd_rn(F.vh, __fmul_rn(F.strat[a], value));
+    const uint32_t rest = (uint32_t)F.vm & ~((2u << a) - 1u);
+    if (!rest) {  // node complete
+      const float vh = F.vh;
+      const long long fv = fix_r(vh, rscale);
+      atomicAdd(row_cnt(tv, F.slot), 1ull << 32);
+      if (touch_row(tv, F.slot, uid, F.vm)) {
+        atomicAdd(row_su(tv, F.slot), (unsigned long long)fv);
+      } else {
+        long long dr[kSlots];
+#pragma unroll
+        for (int b = 0; b < kSlots; ++b) dr[b] = -fv;
+        add_direct(tv, F.slot, F.vm, dr, nullptr);
+      }
+      cnt.updates++;
+      L.value = vh;
+      L.sp--;
       return 0;
     }
-    // sampled opponent: strategy sum, then one action
-    const U4 d = philox(U4{t, uid, (uint32_t)cur.path, (uint32_t)(cur.path >> 32) | 0x80000000u},
-                        G.seed_lo, G.seed_hi);
-    const int s = sample_action(G, reg, vm, uniform01(d.x));
-    if (slot >= 0) {
-      if (touch_row(tv, (unsigned long long)slot, uid, vm)) {
-        atomicAdd(row_cnt(tv, slot), (1ull << 32) | 1ull);
-      } else {
-        atomicAdd(row_cnt(tv, slot), 1ull << 32);
-        float strat[kSlots];
-        node_strategy(reg, vm, strat);
-        long long dw[kSlots];
-#pragma unroll
-        for (int a = 0; a < kSlots; ++a) dw[a] = fix_s(strat[a]);
-        add_direct(tv, slot, vm, nullptr, dw);
-      }
-    }
-    es_apply(G, cur, player, s);
-    cur.depth++;
-    return 0;
-  }
-  // ---- return step: `value` to the top frame
-  if (L.sp == 0) return 1;
-  EsFrame& F = fr.at(L.sp - 1);
-  const int a = F.next_a;
-  const float value = L.value;
-  atomicAdd(row_da(tv, F.slot) + a, (unsigned long long)fix_r(value, rscale));
-  F.vh = __fadd_rn(F.vh, __fmul_rn(F.strat[a], value));
-  const uint32_t rest = (uint32_t)F.vm & ~((2u << a) - 1u);
-  if (rest) {
     const int nx = __ffs(rest) - 1;
     F.next_a = (uint8_t)nx;
     cur = F.st;
-    es_apply(G, cur, F.player, nx);
-    cur.depth++;
+    ap = F.player;
+    aa = nx;
     L.ret = false;
-    return 0;
   }
-  // node complete
-  const float vh = F.vh;
-  const long long fv = fix_r(vh, rscale);
-  atomicAdd(row_cnt(tv, F.slot), 1ull << 32);
-  if (touch_row(tv, F.slot, uid, F.vm)) {
-    atomicAdd(row_su(tv, F.slot), (unsigned long long)fv);
-  } else {
-    long long dr[kSlots];
-#pragma unroll
-    for (int b = 0; b < kSlots; ++b) dr[b] = -fv;
-    add_direct(tv, F.slot, F.vm, dr, nullptr);
-  }
-  cnt.updates++;
-  L.value = vh;
-  L.sp--;
+  es_apply(G, cur, ap, aa);
+  cur.depth++;
   return 0;
 }
 
@@ -382,22 +386,24 @@ k_traverse_es(const GameParams G, const TableView tv, const DealRec* __restrict_
 }
 
 // `work` must be zero when the launch starts; the launch enqueues that reset.
+// The two shallowest frames of each walk live in shared memory (measured best
+// among 0-4 staged frames and probe widths 1-2 on both presets).
 inline void launch_traverse_es(const GameParams& G, const TableView& tv, const DealRec* deals, const Sched* sched,
                                int batch, float rscale, Counters* counters, unsigned* work, cudaStream_t stream) {
-  constexpr int B = 128;
-  static int resident = 0;  // blocks per SM at this kernel's register use
+  constexpr int B = 128, K = 2;
+  constexpr size_t smem = (size_t)K * B * sizeof(EsFrame);
+  static int resident = 0;  // blocks per SM at this kernel's register and shared-memory use
   if (!resident) {
-    // the walk keeps no shared memory: all of it to L1
-    cudaFuncSetAttribute(k_traverse_es<B, 0, 1>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    cudaFuncSetAttribute(k_traverse_es<B, K, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int per_sm = 0, dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_traverse_es<B, 0, 1>, B, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_traverse_es<B, K, 1>, B, smem);
     resident = std::max(1, per_sm) * std::max(1, sms);
   }
   const int grid = std::max(1, std::min(resident, (batch + B - 1) / B));
   cudaMemsetAsync(work, 0, sizeof(unsigned), stream);
-  k_traverse_es<B, 0, 1><<<grid, B, 0, stream>>>(G, tv, deals, sched, batch, rscale, counters, work);
+  k_traverse_es<B, K, 1><<<grid, B, smem, stream>>>(G, tv, deals, sched, batch, rscale, counters, work);
 }
 
 }  // namespace mccfr
