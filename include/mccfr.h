@@ -271,11 +271,11 @@ int mccfr_batch_get_tuning(mccfr_batch* b, mccfr_batch_tuning* t);
 /* Runs `iters` iterations of every table (one CUDA graph per iteration).
    flags bit 1: time every iteration with CUDA events (synchronises per iteration). */
 int mccfr_batch_train(mccfr_batch* b, long long iters, int flags);
-/* Trains one real iteration per candidate tuning (results do not depend on the
-   tuning) and keeps the one with the least traversal-kernel time per node
-   visit; *best receives it.  Candidates: block x grab x
-   smem_frames x warp_sync x probe_width from the sets above, limited to the
-   first `max_candidates` (0 = all 144). */
+/* Trains two real iterations per candidate tuning, the list forward then
+   backward (results do not depend on the tuning), and keeps the candidate with
+   the least summed traversal-kernel time per node visit; *best receives it.
+   Candidates: block x grab x smem_frames x warp_sync x probe_width from the
+   sets above, limited to the first `max_candidates` (0 = all 144). */
 int mccfr_batch_autotune(mccfr_batch* b, int max_candidates, mccfr_batch_tuning* best);
 int mccfr_batch_get_stats(mccfr_batch* b, mccfr_batch_stats* out);
 

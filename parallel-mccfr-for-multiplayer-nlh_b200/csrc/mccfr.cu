@@ -1545,8 +1545,10 @@ int mccfr_batch_autotune(mccfr_batch* b, int max_candidates, mccfr_batch_tuning*
         for (int ws : {1, 0})
           for (int w : {1, 2}) cands.push_back(mccfr_batch_tuning{blk, grab, k, w, ws, {0, 0, 0}});
   if (max_candidates > 0 && (int)cands.size() > max_candidates) cands.resize(max_candidates);
-  // Candidates run on successive real iterations, whose trees shrink as the
-  // strategy sharpens, so they are ranked by traversal-kernel time per node visit.
+  // Candidates run on successive real iterations, whose trees change as the
+  // strategy sharpens; each is ranked by traversal-kernel time per node visit,
+  // summed over a forward and a backward pass through the list so that a
+  // steady drift from one iteration to the next weighs on every candidate alike.
   auto visits_now = [&]() {
     unsigned long long v = 0;
     for (mccfr_handle* h : b->tables) {
@@ -1555,10 +1557,11 @@ int mccfr_batch_autotune(mccfr_batch* b, int max_candidates, mccfr_batch_tuning*
     }
     return v;
   };
-  double best_cost = 1e300;
-  mccfr_batch_tuning best_t = b->tuning;
-  for (const mccfr_batch_tuning& t : cands) {
-    b->tuning = t;
+  std::vector<double> cost(cands.size(), 0.0);
+  const int nc = (int)cands.size();
+  for (int pass = 0; pass < 2 * nc; ++pass) {
+    const int ci = pass < nc ? pass : 2 * nc - 1 - pass;
+    b->tuning = cands[ci];
     const unsigned long long v0 = visits_now();
     int rc = batch_set_scheds(b);
     if (rc) return rc;
@@ -1577,12 +1580,15 @@ int mccfr_batch_autotune(mccfr_batch* b, int max_candidates, mccfr_batch_tuning*
     b->total_ms += it_ms;
     rc = batch_after(b, 1);
     if (rc) return rc;
-    const double cost = trav / (double)std::max(1ull, visits_now() - v0);
-    if (cost < best_cost) {
-      best_cost = cost;
-      best_t = t;
-    }
+    cost[ci] += trav / (double)std::max(1ull, visits_now() - v0);
   }
+  mccfr_batch_tuning best_t = cands[0];
+  double best_cost = cost[0];
+  for (int i = 1; i < nc; ++i)
+    if (cost[i] < best_cost) {
+      best_cost = cost[i];
+      best_t = cands[i];
+    }
   b->tuning = best_t;
   if (b->graph) {
     cudaGraphExecDestroy(b->graph);

@@ -233,7 +233,7 @@ class Batch:
     def autotune(self, max_candidates: int = 0) -> dict:
         best = L.BatchTuning()
         L.check(self._lib.mccfr_batch_autotune(self._b, int(max_candidates), byref(best)))
-        n = len(self.candidates(max_candidates))
+        n = 2 * len(self.candidates(max_candidates))  # forward and backward pass
         for t in self.trainers:
             t.iterations_done += n
         return best.as_dict()

@@ -64,12 +64,12 @@ def test_autotune_keeps_results(hand_table):
     plain = make(cfgs, hand_table)
     batched = make(cfgs, hand_table)
     b = mccfr.Batch(batched, trav)
-    best = b.autotune(max_candidates=6)  # 6 real iterations, one per tuning
+    best = b.autotune(max_candidates=6)  # 12 real iterations: the list forward, then backward
     assert best in mccfr.Batch.candidates(6)
     b.set_tuning(block=64, grab=4, smem_frames=2, probe_width=2, warp_sync=0)
     b.train(1)
     for t, n in zip(plain, trav):
-        t.train(7, n, verbose=False)
+        t.train(13, n, verbose=False)
     for p, q in zip(plain, batched):
         rows_equal(p.export_rows(), q.export_rows())
     b.close()
