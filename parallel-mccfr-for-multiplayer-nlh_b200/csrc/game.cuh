@@ -34,6 +34,7 @@ struct GameParams {
   uint8_t fallback[kSlots];
   uint8_t default_slot;
   int stack_base;  // chips behind plus chips already in: stack + (subgame) pot share
+  int8_t den_shift[kSlots];  // log2(den[a]) when den[a] is a power of two, else -1
 };
 
 // ---------------------------------------------------------------------------
@@ -113,7 +114,9 @@ __host__ __device__ __forceinline__ int min_raise_to(int cb, int lfr, int bb) {
 
 __host__ __device__ __forceinline__ int raise_target(const GameParams& G, int a, int pot, int cb, int mrt) {
   if (G.kind[a] == 4 /*RAISE_MIN*/) return mrt;
-  const int frac = (G.num[a] * pot) / G.den[a];
+  // num * pot >= 0, so a power-of-two denominator is an exact shift
+  const int x = G.num[a] * pot, sh = G.den_shift[a];
+  const int frac = sh >= 0 ? (x >> sh) : x / G.den[a];
   return imax(mrt, cb + imax(1, frac));
 }
 

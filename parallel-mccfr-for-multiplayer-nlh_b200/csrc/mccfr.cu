@@ -403,6 +403,9 @@ void make_params(const mccfr_config& c, GameParams& g) {
     g.kind[a] = (int8_t)(a < c.num_actions ? c.action_kind[a] : -1);
     g.num[a] = (int16_t)(a < c.num_actions ? c.action_num[a] : 0);
     g.den[a] = (int16_t)(a < c.num_actions ? std::max(1, c.action_den[a]) : 1);
+    g.den_shift[a] = -1;
+    for (int k = 0; k < 15; ++k)
+      if (g.den[a] == (1 << k)) g.den_shift[a] = (int8_t)k;
     const int k = g.kind[a];
     if (k == MCCFR_ACT_FOLD) g.m_fold |= 1u << a;
     if (k == MCCFR_ACT_CHECK || k == MCCFR_ACT_CHECK_CALL) g.m_check |= 1u << a;
