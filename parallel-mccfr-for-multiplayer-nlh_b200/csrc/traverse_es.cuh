@@ -179,6 +179,19 @@ __device__ __forceinline__ void es_begin(const GameParams& G, const DealRec* D, 
 
 }
 
+// Kind of a traversal's next event, without doing it: 0 opponent visit, 1
+// updating-player visit, 2 return to a frame, 3 showdown, 4 a cheap step
+// (depth cut, fold terminal or street change).
+__device__ __forceinline__ int es_peek(const GameParams& G, const EsLane& L, int up) {
+  if (L.ret) return 2;
+  const EsState& cur = L.cur;
+  if (cur.depth >= G.max_depth) return 4;
+  const uint32_t live = ((1u << G.N) - 1) & ~(uint32_t)cur.folded;
+  if (__popc(live) == 1) return 4;
+  if (cur.nq == 0) return cur.street < 3 ? 4 : 3;
+  return (int)(cur.q & 0xF) == up ? 1 : 0;
+}
+
 // One event of a traversal: a descend step (one decision node, a street change
 // or a terminal) or a return step (one child value handed to the top frame).
 // Returns 0 while the traversal goes on, 1 when it is complete, 2 when it
@@ -357,6 +370,8 @@ k_traverse_es(const GameParams G, const TableView tv, const DealRec* __restrict_
   const int lane = threadIdx.x & 31;
   EsLane L;
   bool have = false, more = true;
+  constexpr int kMaxWait = 4;
+  int waited = 0;
   // The whole warp stays in the loop until every lane is out of work, and
   // reconverges before each event.
   for (;;) {
@@ -380,7 +395,28 @@ k_traverse_es(const GameParams G, const TableView tv, const DealRec* __restrict_
       }
     }
     if (!__any_sync(0xFFFFFFFFu, have)) break;
-    if (have && es_step<W>(G, tv, uid, up, rscale, fr, L, c)) have = false;
+    // Event-kind scheduling: of the expensive kinds, the warp runs the one most
+    // lanes wait for (cheap steps run for everyone), so more lanes share each
+    // issued instruction; a lane that has waited kMaxWait iterations forces its
+    // kind.  Each lane's own sequence of events is unchanged.
+    const int ty = have ? es_peek(G, L, up) : -1;
+    int pick = 0, best = -1;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int n = __popc(__ballot_sync(0xFFFFFFFFu, ty == k));
+      if (n > best) {
+        best = n;
+        pick = k;
+      }
+    }
+    const unsigned forced = __ballot_sync(0xFFFFFFFFu, have && ty < 4 && waited >= kMaxWait);
+    if (forced) pick = __shfl_sync(0xFFFFFFFFu, ty, __ffs(forced) - 1);
+    if (have && (ty == pick || ty == 4)) {
+      waited = 0;
+      if (es_step<W>(G, tv, uid, up, rscale, fr, L, c)) have = false;
+    } else if (have) {
+      waited++;
+    }
   }
   warp_add_counters(counters, trav, c.visits, c.updates, c.terminals, trav * (unsigned)G.N);
 }
