@@ -191,12 +191,15 @@ int mccfr_step(mccfr_handle* h, long long iteration, int player, int batch,
 /* Normalised average strategy, one row per info-set key with a non-zero sum,
    sorted by key.  keys[i] is the reference's u32 dump key (the FNV slot) in
    FNV26 mode and the low 32 bits of the 64-bit key otherwise; keys64 (optional)
-   receives full keys.  probs is [capacity][8]. */
+   receives full keys.  probs is [capacity][8].  capacity 0 is a size query:
+   *count receives the number of occupied rows, an upper bound of the rows
+   written (MCCFR_ERR_CAPACITY when it is not 0). */
 int mccfr_get_strategy(mccfr_handle* h, uint32_t* keys, uint64_t* keys64,
                        float* probs, size_t capacity, size_t* count);
 int mccfr_num_info_sets_active(mccfr_handle* h, long long* out);
 /* Every occupied row, sorted by key: regrets [8], strategy sums [8] and the
-   number of updates the row received. */
+   number of updates the row received.  capacity 0 is a size query (a counting
+   pass; MCCFR_ERR_CAPACITY with *count = rows when there are any). */
 int mccfr_export_rows(mccfr_handle* h, uint64_t* keys, float* regrets,
                       float* strategy_sum, uint64_t* visits, size_t capacity,
                       size_t* count);

@@ -140,15 +140,27 @@ __global__ void k_advance_batched(const TableDesc* __restrict__ tables, const Ph
   D.sched->player = p;
 }
 
+// Occupied rows of the table (one atomic per warp).
+__global__ void k_count_rows(const TableView tv, unsigned long long cap_slots, unsigned int* __restrict__ on) {
+  unsigned c = 0;
+  for (unsigned long long s = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; s < cap_slots;
+       s += (unsigned long long)gridDim.x * blockDim.x)
+    c += *row_key(tv, s) != 0;
+  c = __reduce_add_sync(0xFFFFFFFFu, c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(on, c);
+}
+
+// Compacts the occupied rows into arrays of `bound` rows (unordered).
 __global__ void k_export(const TableView tv, unsigned long long cap_slots,
                          unsigned long long* __restrict__ okeys, float4* __restrict__ oreg,
                          float4* __restrict__ ossum, unsigned long long* __restrict__ ovis,
-                         unsigned int* __restrict__ on) {
+                         unsigned int* __restrict__ on, unsigned bound) {
   for (unsigned long long s = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; s < cap_slots;
        s += (unsigned long long)gridDim.x * blockDim.x) {
     const unsigned long long k = *row_key(tv, s);
     if (!k) continue;
     const unsigned i = atomicAdd(on, 1u);
+    if (i >= bound) continue;
     okeys[i] = k;
     oreg[2 * i] = row_reg(tv, s)[0];
     oreg[2 * i + 1] = row_reg(tv, s)[1];
@@ -552,57 +564,66 @@ struct HostRow {
   unsigned long long visits;
 };
 
-int read_rows(mccfr_handle* h, std::vector<HostRow>& rows) {
+// Occupied rows (a counting pass over the table).
+int count_rows(mccfr_handle* h, unsigned int* n) {
   CK(cudaStreamSynchronize(h->stream));
   unsigned int* d_n = nullptr;
   CK(cudaMalloc(&d_n, sizeof(unsigned int)));
-  CK(cudaMemset(d_n, 0, sizeof(unsigned int)));
-  unsigned long long *okeys = nullptr, *ovis = nullptr;
-  float4 *oreg = nullptr, *ossum = nullptr;
-  // One pass into buffers bounded by the capacity.
-  const unsigned long long bound = h->cap;
-  cudaError_t e = cudaMalloc(&okeys, bound * sizeof(unsigned long long));
-  if (e == cudaSuccess) e = cudaMalloc(&ovis, bound * sizeof(unsigned long long));
-  if (e == cudaSuccess) e = cudaMalloc(&oreg, bound * 2 * sizeof(float4));
-  if (e == cudaSuccess) e = cudaMalloc(&ossum, bound * 2 * sizeof(float4));
-  int rc = MCCFR_OK;
-  unsigned int n = 0;
-  if (e != cudaSuccess) {
-    rc = fail(h, MCCFR_ERR_OOM, "export buffers: %s", cudaGetErrorString(e));
-  } else {
-    k_export<<<148 * 16, 256, 0, h->stream>>>(h->tv, h->cap, okeys, oreg, ossum, ovis, d_n);
-    e = cudaMemcpyAsync(&n, d_n, sizeof(n), cudaMemcpyDeviceToHost, h->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    if (e != cudaSuccess) rc = fail(h, MCCFR_ERR_CUDA, "export: %s", cudaGetErrorString(e));
-    if (rc == MCCFR_OK) {
-      std::vector<unsigned long long> k(n), v(n);
-      std::vector<float> r(8ull * n), s(8ull * n);
-      if (n) {
-        e = cudaMemcpy(k.data(), okeys, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
-        if (e == cudaSuccess) e = cudaMemcpy(v.data(), ovis, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
-        if (e == cudaSuccess) e = cudaMemcpy(r.data(), oreg, n * 32ull, cudaMemcpyDeviceToHost);
-        if (e == cudaSuccess) e = cudaMemcpy(s.data(), ossum, n * 32ull, cudaMemcpyDeviceToHost);
-      }
-      if (e != cudaSuccess) {
-        rc = fail(h, MCCFR_ERR_CUDA, "export copy: %s", cudaGetErrorString(e));
-      } else {
-        rows.resize(n);
-        for (unsigned i = 0; i < n; ++i) {
-          rows[i].key = k[i];
-          std::memcpy(rows[i].reg, &r[8ull * i], 32);
-          std::memcpy(rows[i].ssum, &s[8ull * i], 32);
-          rows[i].visits = v[i];
-        }
-        std::sort(rows.begin(), rows.end(), [](const HostRow& a, const HostRow& b) { return a.key < b.key; });
-      }
-    }
+  cudaError_t e = cudaMemsetAsync(d_n, 0, sizeof(unsigned int), h->stream);
+  if (e == cudaSuccess) {
+    k_count_rows<<<148 * 16, 256, 0, h->stream>>>(h->tv, h->cap, d_n);
+    e = cudaMemcpyAsync(n, d_n, sizeof(unsigned int), cudaMemcpyDeviceToHost, h->stream);
   }
-  cudaFree(okeys);
-  cudaFree(ovis);
-  cudaFree(oreg);
-  cudaFree(ossum);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   cudaFree(d_n);
-  return rc;
+  if (e != cudaSuccess) return fail(h, MCCFR_ERR_CUDA, "row count: %s", cudaGetErrorString(e));
+  return MCCFR_OK;
+}
+
+// Every occupied row, sorted by key: counted first, then compacted into
+// buffers of exactly that many rows and copied back.
+int read_rows(mccfr_handle* h, std::vector<HostRow>& rows) {
+  unsigned int n = 0;
+  int rc = count_rows(h, &n);
+  if (rc) return rc;
+  rows.clear();
+  if (n == 0) return MCCFR_OK;
+  void* block = nullptr;
+  const size_t bytes = (size_t)n * (8 + 8 + 32 + 32) + 256;
+  cudaError_t e = cudaMalloc(&block, bytes);
+  if (e != cudaSuccess) return fail(h, MCCFR_ERR_OOM, "export buffers: %s", cudaGetErrorString(e));
+  char* base = static_cast<char*>(block);
+  float4* oreg = reinterpret_cast<float4*>(base);
+  float4* ossum = reinterpret_cast<float4*>(base + (size_t)n * 32);
+  unsigned long long* okeys = reinterpret_cast<unsigned long long*>(base + (size_t)n * 64);
+  unsigned long long* ovis = reinterpret_cast<unsigned long long*>(base + (size_t)n * 72);
+  unsigned int* d_n = reinterpret_cast<unsigned int*>(base + (size_t)n * 80);
+  std::vector<unsigned long long> k(n), v(n);
+  std::vector<float> r(8ull * n), s(8ull * n);
+  e = cudaMemsetAsync(d_n, 0, sizeof(unsigned int), h->stream);
+  if (e == cudaSuccess) {
+    k_export<<<148 * 16, 256, 0, h->stream>>>(h->tv, h->cap, okeys, oreg, ossum, ovis, d_n, n);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(k.data(), okeys, n * 8ull, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(v.data(), ovis, n * 8ull, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(r.data(), oreg, n * 32ull, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(s.data(), ossum, n * 32ull, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(block);
+  if (e != cudaSuccess) return fail(h, MCCFR_ERR_CUDA, "export: %s", cudaGetErrorString(e));
+  std::vector<unsigned> order(n);
+  for (unsigned i = 0; i < n; ++i) order[i] = i;
+  std::sort(order.begin(), order.end(), [&k](unsigned a, unsigned b) { return k[a] < k[b]; });
+  rows.resize(n);
+  for (unsigned j = 0; j < n; ++j) {
+    const unsigned i = order[j];
+    rows[j].key = k[i];
+    std::memcpy(rows[j].reg, &r[8ull * i], 32);
+    std::memcpy(rows[j].ssum, &s[8ull * i], 32);
+    rows[j].visits = v[i];
+  }
+  return MCCFR_OK;
 }
 
 void release(mccfr_handle* h) {
@@ -1038,6 +1059,12 @@ int mccfr_export_rows(mccfr_handle* h, uint64_t* keys, float* regrets, float* st
                       size_t capacity, size_t* count) {
   if (!h || !count) return MCCFR_ERR_INVALID_ARG;
   CK(cudaSetDevice(h->device));
+  if (capacity == 0) {  // size query: a counting pass only
+    unsigned int n = 0;
+    const int rc = count_rows(h, &n);
+    *count = n;
+    return rc ? rc : (n ? MCCFR_ERR_CAPACITY : MCCFR_OK);
+  }
   std::vector<HostRow> rows;
   const int rc = read_rows(h, rows);
   if (rc) return rc;
@@ -1057,6 +1084,12 @@ int mccfr_get_strategy(mccfr_handle* h, uint32_t* keys, uint64_t* keys64, float*
                        size_t* count) {
   if (!h || !count) return MCCFR_ERR_INVALID_ARG;
   CK(cudaSetDevice(h->device));
+  if (capacity == 0) {  // size query: occupied rows, an upper bound of the rows written
+    unsigned int n = 0;
+    const int rc = count_rows(h, &n);
+    *count = n;
+    return rc ? rc : (n ? MCCFR_ERR_CAPACITY : MCCFR_OK);
+  }
   std::vector<HostRow> rows;
   const int rc = read_rows(h, rows);
   if (rc) return rc;

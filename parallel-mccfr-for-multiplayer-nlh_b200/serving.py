@@ -145,6 +145,8 @@ class ReSolveServer:
         self.tuning = tuning
         self.free_memory = free_memory or self._device_free
         self.rounds = 0
+        # host seconds spent admitting (table creation), in rounds, and retiring
+        self.timing = {"admit_s": 0.0, "round_s": 0.0, "retire_s": 0.0}
 
     @staticmethod
     def _device_free() -> int:
@@ -175,16 +177,21 @@ class ReSolveServer:
             now = time.perf_counter() - t0
             while pending and (not realtime or pending[0].arrival <= now):
                 queue.append(pending.pop(0))
+            ta = time.perf_counter()
             while queue and self.admit_ok(queue[0], held, len(active)):
                 req = queue.pop(0)
                 active.append(self._start(req, time.perf_counter() - t0))
                 held += table_bytes(req)
+            self.timing["admit_s"] += time.perf_counter() - ta
             if not active:
                 if pending:
                     time.sleep(max(0.0, min(0.001, pending[0].arrival - now)))
                 continue
+            tr = time.perf_counter()
             batch_round([s.trainer for s in active], [self.traversals] * len(active), self.tuning)
             self.rounds += 1
+            tz = time.perf_counter()
+            self.timing["round_s"] += tz - tr
             still = []
             for s in active:
                 s.updates_done += 1
@@ -196,6 +203,7 @@ class ReSolveServer:
                 else:
                     still.append(s)
             active = still
+            self.timing["retire_s"] += time.perf_counter() - tz
         return results
 
 
