@@ -307,7 +307,9 @@ def serving_sweep(m, L, table, rates=(10, 30, 100, 300, 1000), n_requests=48) ->
             r.arrival = float(a)
         srv = sv.ReSolveServer(owner, hbm_budget=32 << 30, traversals=1024)
         res = srv.run(reqs)
-        out[f"lambda_{rate}"] = {**sv.summarize(res), "rounds": srv.rounds}
+        out[f"lambda_{rate}"] = {**sv.summarize(res), "rounds": srv.rounds, "tables_reused": srv.reused,
+                                 **{k: round(v, 3) for k, v in srv.timing.items()}}
+        srv.close()
     owner.close()
     out["workload"] = (f"{n_requests} requests per rate: turn/river board, 2-6 players, pot U[2,200]BB, "
                        "Dirichlet(0.5) ranges, 3-5 sizes + all-in, budget log-uniform [2e3,5e4] traversals per "

@@ -299,6 +299,11 @@ typedef struct mccfr_subgame {
   const float* ranges;    /* [num_players][1326] non-negative weights */
 } mccfr_subgame;
 int mccfr_create_subgame(const mccfr_config* cfg, const mccfr_subgame* sg, mccfr_handle** out);
+/* Re-targets a subgame handle to a new subgame, as if it had just been created
+   with (cfg, sg): same table capacity (cfg->table_log2) and device; everything
+   else may differ.  The table is zeroed and the allocations are kept, so a
+   server can reuse finished requests' tables without freeing and allocating. */
+int mccfr_subgame_reset(mccfr_handle* h, const mccfr_config* cfg, const mccfr_subgame* sg);
 /* Makes h use src's device rank table instead of uploading its own (src must
    outlive h).  Valid for subgames and for tables without rank-CDF buckets or
    with the same bucket counts as src. */

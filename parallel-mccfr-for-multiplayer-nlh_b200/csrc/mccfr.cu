@@ -291,6 +291,7 @@ struct mccfr_handle {
   unsigned long long cap = 0;
   TableView tv{};
   void* d_block = nullptr;  // one allocation for the table arrays
+  size_t block_bytes = 0;
   Sched* d_sched = nullptr;
   DealRec* d_deals = nullptr;  // one record per traversal of an update
   int deals_cap = 0;
@@ -815,6 +816,7 @@ int mccfr_create(const mccfr_config* cfg, mccfr_handle** out) {
   h->cap = 1ull << cfg->table_log2;
   const unsigned long long C = h->cap;
   const size_t bytes_rows = C * kRowBytes, bytes_touch = C * 4, bytes_misc = 256;
+  h->block_bytes = bytes_rows + bytes_touch + bytes_misc;
   CKC(cudaMalloc(&h->d_block, bytes_rows + bytes_touch + bytes_misc));
   CKC(cudaMemset(h->d_block, 0, bytes_rows + bytes_touch + bytes_misc));
   char* base = static_cast<char*>(h->d_block);
@@ -1708,14 +1710,20 @@ bool build_range_cdf(const float* w, uint64_t board_mask, uint32_t* out) {
 
 extern "C" {
 
-int mccfr_create_subgame(const mccfr_config* cfg, const mccfr_subgame* sg, mccfr_handle** out) {
-  if (!cfg || !sg || !out || !sg->ranges) return MCCFR_ERR_INVALID_ARG;
+}  // extern "C"
+
+namespace {
+
+// Checks a subgame against its config and builds each player's range CDF.
+int subgame_cdfs(const mccfr_config* cfg, const mccfr_subgame* sg, std::vector<uint32_t>& cdf, int& nb) {
+  if (!cfg || !sg || !sg->ranges) return MCCFR_ERR_INVALID_ARG;
   if (cfg->key_mode != MCCFR_KEY_ID64) {
-    fprintf(stderr, "mccfr_create_subgame: subgames use ID64 keys\n");
+    fprintf(stderr, "subgame: subgames use ID64 keys\n");
     return MCCFR_ERR_INVALID_ARG;
   }
   if (sg->street != 2 && sg->street != 3) return MCCFR_ERR_INVALID_ARG;
-  const int nb = sg->street == 2 ? 4 : 5;
+  if (cfg->num_players < 2 || cfg->num_players > MCCFR_MAX_PLAYERS) return MCCFR_ERR_INVALID_ARG;
+  nb = sg->street == 2 ? 4 : 5;
   uint64_t mask = 0;
   for (int i = 0; i < nb; ++i) {
     if (sg->board[i] > 51 || ((mask >> sg->board[i]) & 1)) return MCCFR_ERR_INVALID_ARG;
@@ -1724,26 +1732,82 @@ int mccfr_create_subgame(const mccfr_config* cfg, const mccfr_subgame* sg, mccfr
   // invested chips are 16-bit: a player's pot share plus its whole stack must fit
   if (sg->pot < 0 || sg->pot % cfg->num_players != 0 || sg->pot / cfg->num_players + cfg->starting_stack > 65535)
     return MCCFR_ERR_INVALID_ARG;
-  std::vector<uint32_t> cdf((size_t)cfg->num_players * 1326);
+  cdf.assign((size_t)cfg->num_players * 1326, 0);
   for (int p = 0; p < cfg->num_players; ++p)
     if (!build_range_cdf(sg->ranges + 1326 * p, mask, cdf.data() + 1326 * p)) {
-      fprintf(stderr, "mccfr_create_subgame: player %d's range has no weight off the board\n", p);
+      fprintf(stderr, "subgame: player %d's range has no weight off the board\n", p);
       return MCCFR_ERR_INVALID_ARG;
     }
-  const int rc = mccfr_create(cfg, out);
-  if (rc) return rc;
-  mccfr_handle* h = *out;
-  if (cudaMalloc(&h->d_ranges, cdf.size() * 4) != cudaSuccess ||
-      cudaMemcpy(h->d_ranges, cdf.data(), cdf.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
-    mccfr_destroy(h);
-    *out = nullptr;
-    return MCCFR_ERR_OOM;
-  }
+  return MCCFR_OK;
+}
+
+void set_subgame_params(mccfr_handle* h, const mccfr_config* cfg, const mccfr_subgame* sg, int nb) {
   h->gp.sub_street = sg->street;
   h->gp.sub_pot = sg->pot;
   h->gp.stack_base = cfg->starting_stack + sg->pot / cfg->num_players;
   for (int i = 0; i < 5; ++i) h->gp.sub_board[i] = (i < nb) ? sg->board[i] : 0;
   h->gp.range_cdf = h->d_ranges;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mccfr_create_subgame(const mccfr_config* cfg, const mccfr_subgame* sg, mccfr_handle** out) {
+  if (!out) return MCCFR_ERR_INVALID_ARG;
+  std::vector<uint32_t> cdf;
+  int nb = 0;
+  int rc = subgame_cdfs(cfg, sg, cdf, nb);
+  if (rc) return rc;
+  rc = mccfr_create(cfg, out);
+  if (rc) return rc;
+  mccfr_handle* h = *out;
+  // room for any player count, so a reset can take a different one
+  if (cudaMalloc(&h->d_ranges, (size_t)MCCFR_MAX_PLAYERS * 1326 * 4) != cudaSuccess ||
+      cudaMemcpy(h->d_ranges, cdf.data(), cdf.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+    mccfr_destroy(h);
+    *out = nullptr;
+    return MCCFR_ERR_OOM;
+  }
+  set_subgame_params(h, cfg, sg, nb);
+  return MCCFR_OK;
+}
+
+int mccfr_subgame_reset(mccfr_handle* h, const mccfr_config* cfg, const mccfr_subgame* sg) {
+  if (!h || !cfg || !sg) return MCCFR_ERR_INVALID_ARG;
+  if (!h->gp.sub_street || !h->d_ranges) return fail(h, MCCFR_ERR_INVALID_ARG, "not a subgame handle");
+  if (cfg->table_log2 != h->cfg.table_log2 || cfg->device != h->cfg.device)
+    return fail(h, MCCFR_ERR_INVALID_ARG, "a reset keeps the table capacity and device");
+  std::string why;
+  if (validate(*cfg, why)) return fail(h, MCCFR_ERR_INVALID_ARG, "%s", why.c_str());
+  std::vector<uint32_t> cdf;
+  int nb = 0;
+  const int rc = subgame_cdfs(cfg, sg, cdf, nb);
+  if (rc) return fail(h, rc, "invalid subgame");
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  uint8_t pre[52 * 52];
+  build_preflop_lut(cfg->preflop_mode, cfg->preflop_buckets, pre);
+  CK(cudaMemcpyAsync(h->d_pre, pre, sizeof(pre), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_ranges, cdf.data(), cdf.size() * 4, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemsetAsync(h->d_block, 0, h->block_bytes, h->stream));  // rows, touched list, counters
+  CK(cudaMemsetAsync(h->d_counters, 0, sizeof(Counters), h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->cfg = *cfg;
+  make_params(*cfg, h->gp);
+  set_subgame_params(h, cfg, sg, nb);
+  if (h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  h->graph_batch = -1;
+  h->iterations_done = 0;
+  h->launches = 0;
+  h->round_player = 0;
+  h->traverse_ms = h->apply_ms = h->last_traverse_ms = h->last_apply_ms = 0;
+  h->touched_last = 0;
+  h->sticky_err = 0;
+  h->last_error.clear();
   return MCCFR_OK;
 }
 

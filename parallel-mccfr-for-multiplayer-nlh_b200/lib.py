@@ -160,6 +160,7 @@ SIGNATURES = {
     "mccfr_share_hand_table": (c_int, [c_void_p, c_void_p]),
     "mccfr_batch_round": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
     "mccfr_get_progress": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mccfr_subgame_reset": (c_int, [c_void_p, c_void_p, c_void_p]),
     "mccfr_br_options_init": (None, [c_void_p]),
     "mccfr_best_response": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p, c_size_t,
                                     c_void_p, c_void_p]),

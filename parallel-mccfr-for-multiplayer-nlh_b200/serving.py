@@ -131,10 +131,14 @@ class Result:
 class ReSolveServer:
     """Continuous-batching re-solver.
 
-    hbm_budget: device bytes the server may hold in request tables (admission
-    also requires that much free device memory); max_active: requests batched
-    per round (the persistent kernel takes up to 64 tables); traversals: per
-    player-update of each request."""
+    hbm_budget: device bytes the server may hold in request tables, pooled ones
+    included (admission also requires that much free device memory);
+    max_active: requests batched per round (the persistent kernel takes up to 64
+    tables); traversals: per player-update of each request.  Finished requests'
+    tables are kept in a pool by capacity and reset for new requests of the
+    same capacity (mccfr_subgame_reset), so a steady stream of requests
+    allocates and frees no device memory; pooled tables are freed when a new
+    capacity needs the room, and by close()."""
 
     def __init__(self, rank_table_owner: GPUCFRTrainer, hbm_budget: int = 16 << 30, max_active: int = 64,
                  traversals: int = 256, tuning: dict | None = None, free_memory=None):
@@ -147,6 +151,8 @@ class ReSolveServer:
         self.rounds = 0
         # host seconds spent admitting (table creation), in rounds, and retiring
         self.timing = {"admit_s": 0.0, "round_s": 0.0, "retire_s": 0.0}
+        self.pool: dict[int, list[GPUCFRTrainer]] = {}
+        self.reused = 0
 
     @staticmethod
     def _device_free() -> int:
@@ -154,15 +160,43 @@ class ReSolveServer:
 
         return int(torch.cuda.mem_get_info()[0])
 
+    def pooled_bytes(self) -> int:
+        return sum((1 << log2) * (256 + 4) + (1 << 20) for log2, ts in self.pool.items() for _ in ts)
+
+    def _evict(self, need: int, held: int) -> None:
+        """Frees pooled tables of other capacities until `need` more bytes fit."""
+        for log2 in sorted(self.pool, key=lambda k: -k):
+            while self.pool[log2] and held + self.pooled_bytes() + need > self.hbm_budget:
+                self.pool[log2].pop().close()
+
     def admit_ok(self, req: Request, held: int, n_active: int) -> bool:
+        if n_active >= self.max_active:
+            return False
+        if self.pool.get(req.table_log2):
+            return True  # a pooled table of this capacity is reset, nothing is allocated
         need = table_bytes(req)
-        return n_active < self.max_active and held + need <= self.hbm_budget and need + (1 << 30) <= self.free_memory()
+        self._evict(need, held)
+        return held + self.pooled_bytes() + need <= self.hbm_budget and need + (1 << 30) <= self.free_memory()
 
     def _start(self, req: Request, now: float) -> Solve:
-        t = GPUCFRTrainer.subgame(request_config(req), req.street, req.pot, req.board, req.ranges)
-        t.share_hand_table(self.owner)
+        cfg = request_config(req)
+        ts = self.pool.get(req.table_log2)
+        if ts:
+            t = ts.pop()
+            t.reset_subgame(cfg, req.street, req.pot, req.board, req.ranges)
+            self.reused += 1
+        else:
+            t = GPUCFRTrainer.subgame(cfg, req.street, req.pot, req.board, req.ranges)
+            t.share_hand_table(self.owner)
         per_player = max(1, math.ceil(req.budget / self.traversals))
         return Solve(req, t, per_player * req.players, admitted=now)
+
+    def close(self) -> None:
+        """Frees the pooled tables."""
+        for ts in self.pool.values():
+            for t in ts:
+                t.close()
+        self.pool.clear()
 
     def run(self, requests: list[Request], realtime: bool = True) -> list[Result]:
         """Serves requests in arrival order; with realtime=False arrivals are
@@ -198,7 +232,7 @@ class ReSolveServer:
                 if s.updates_done >= s.updates_needed:
                     keys, probs = s.trainer.strategy_arrays()
                     results.append(Result(s.req.rid, s.req.arrival, s.admitted, time.perf_counter() - t0, keys, probs))
-                    s.trainer.close()
+                    self.pool.setdefault(s.req.table_log2, []).append(s.trainer)  # kept for the next request
                     held -= table_bytes(s.req)
                 else:
                     still.append(s)

@@ -65,6 +65,15 @@ class GPUCFRTrainer:
         self.iterations_done = 0
         return self
 
+    def reset_subgame(self, config: L.Config, street: int, pot: int, board, ranges: np.ndarray) -> None:
+        """Re-targets this subgame trainer to a new subgame with the same table
+        capacity (mccfr_subgame_reset): as if freshly created, allocations kept."""
+        sg, _keep = L.subgame_struct(street, pot, board,
+                                     np.asarray(ranges, dtype=np.float32).reshape(config.num_players, 1326))
+        L.check(self._lib.mccfr_subgame_reset(self._h, byref(config), byref(sg)), self._h)
+        self.config = config
+        self.iterations_done = 0
+
     def share_hand_table(self, src: "GPUCFRTrainer") -> None:
         L.check(self._lib.mccfr_share_hand_table(self._h, src.handle), self._h)
 

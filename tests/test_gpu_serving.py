@@ -83,3 +83,28 @@ def test_each_request_same_alone_and_mixed(hand_table):
         alone = sv.ReSolveServer(owner, traversals=128).run([req], realtime=False)[0]
         assert np.array_equal(alone.keys, out[req.rid].keys)
         assert np.array_equal(alone.probs.view(np.uint32), out[req.rid].probs.view(np.uint32))
+
+
+def test_reset_table_equals_fresh_table(hand_table):
+    """A subgame trainer reset to another subgame (mccfr_subgame_reset) trains
+    exactly like a trainer created for that subgame."""
+    sv = serving()
+    owner = mccfr.GPUCFRTrainer(config=L.preset(L.PRESET_HU_20BB), table_log2=10)
+    owner.set_hand_table(hand_table)
+    a = small_request(11, 3, 4)
+    b = small_request(12, 2, 3)
+    b.table_log2 = a.table_log2
+    ca, cb = sv.request_config(a), sv.request_config(b)
+    reused = mccfr.GPUCFRTrainer.subgame(ca, a.street, a.pot, a.board, a.ranges)
+    reused.share_hand_table(owner)
+    reused.train(2, 512, verbose=False)
+    reused.reset_subgame(cb, b.street, b.pot, b.board, b.ranges)
+    fresh = mccfr.GPUCFRTrainer.subgame(cb, b.street, b.pot, b.board, b.ranges)
+    fresh.share_hand_table(owner)
+    for t in (reused, fresh):
+        t.train(2, 512, verbose=False)
+        mccfr.batch_round([t], [256])
+    rows_equal(reused.export_rows(), fresh.export_rows())
+    assert reused.progress() == fresh.progress()
+    for t in (reused, fresh, owner):
+        t.close()

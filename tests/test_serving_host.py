@@ -53,3 +53,32 @@ def test_poisson_arrivals_rate():
     a = sv.poisson_arrivals(rng, 20000, 100.0)
     assert np.all(np.diff(a) > 0)
     assert abs(20000 / a[-1] - 100.0) < 3.0
+
+
+class _FakeTrainer:
+    def __init__(self):
+        self.closed = False
+
+    def close(self):
+        self.closed = True
+
+
+def test_pool_reuse_and_eviction():
+    """A pooled table of the request's capacity is reused with nothing
+    allocated; tables of other capacities are freed when room is needed."""
+    rng = np.random.default_rng(3)
+    req = sv.make_request(rng, 0)
+    need = sv.table_bytes(req)
+    srv = sv.ReSolveServer(None, hbm_budget=2 * need, free_memory=lambda: 100 << 30)
+    same = _FakeTrainer()
+    srv.pool[req.table_log2] = [same]
+    assert srv.admit_ok(req, 2 * need, 0)        # full budget, but the pooled table is reused
+    other = _FakeTrainer()
+    other_log2 = req.table_log2 - 1 if req.table_log2 > 14 else req.table_log2 + 1
+    srv.pool = {other_log2: [other]}
+    assert srv.admit_ok(req, need, 0)             # the other-capacity table is freed to make room
+    assert other.closed and not srv.pool[other_log2]
+    srv.pool = {other_log2: [_FakeTrainer()]}
+    assert not srv.admit_ok(req, 2 * need, 0)     # no room even with the pool empty
+    srv.close()
+    assert srv.pool == {}
