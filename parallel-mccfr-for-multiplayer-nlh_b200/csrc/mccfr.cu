@@ -581,6 +581,29 @@ int count_rows(mccfr_handle* h, unsigned int* n) {
   return MCCFR_OK;
 }
 
+// Indices of `k` in ascending key order: LSD radix sort, 8 bits per pass,
+// skipping the bytes in which all keys agree (keys are distinct).
+void order_by_key(const std::vector<unsigned long long>& k, std::vector<unsigned>& order) {
+  const size_t n = k.size();
+  order.resize(n);
+  for (size_t i = 0; i < n; ++i) order[i] = (unsigned)i;
+  unsigned long long orv = 0, andv = ~0ull;
+  for (unsigned long long x : k) {
+    orv |= x;
+    andv &= x;
+  }
+  const unsigned long long vary = orv ^ andv;
+  std::vector<unsigned> tmp(n);
+  for (int sh = 0; sh < 64; sh += 8) {
+    if (((vary >> sh) & 0xFF) == 0) continue;
+    size_t cnt[257] = {0};
+    for (size_t i = 0; i < n; ++i) cnt[((k[order[i]] >> sh) & 0xFF) + 1]++;
+    for (int b = 0; b < 256; ++b) cnt[b + 1] += cnt[b];
+    for (size_t i = 0; i < n; ++i) tmp[cnt[(k[order[i]] >> sh) & 0xFF]++] = order[i];
+    order.swap(tmp);
+  }
+}
+
 // Every occupied row, sorted by key: counted first, then compacted into
 // buffers of exactly that many rows and copied back.
 int read_rows(mccfr_handle* h, std::vector<HostRow>& rows) {
@@ -613,9 +636,8 @@ int read_rows(mccfr_handle* h, std::vector<HostRow>& rows) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   cudaFree(block);
   if (e != cudaSuccess) return fail(h, MCCFR_ERR_CUDA, "export: %s", cudaGetErrorString(e));
-  std::vector<unsigned> order(n);
-  for (unsigned i = 0; i < n; ++i) order[i] = i;
-  std::sort(order.begin(), order.end(), [&k](unsigned a, unsigned b) { return k[a] < k[b]; });
+  std::vector<unsigned> order;
+  order_by_key(k, order);
   rows.resize(n);
   for (unsigned j = 0; j < n; ++j) {
     const unsigned i = order[j];
