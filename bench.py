@@ -513,7 +513,8 @@ def main():
         "config": {**describe(cfg, args.workload, batch), "parallelism": f"replicas{world}"},
         "e2e": {"value": e2e_value, "unit": "traversals/s", "h2d_bytes_per_step": 16,
                 "d2h_bytes_per_step": 44},
-        "gpu_launches": int(args.steps * cfg.num_players * 3),
+        # per player-update: k_deal, the traversal kernel, k_apply, k_advance
+        "gpu_launches": int(args.steps * cfg.num_players * 4),
         "clocks": clocks.summary(),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic, "peak_kind": peak_kind,
