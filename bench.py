@@ -360,6 +360,53 @@ def hu_subgame_exploitability(m, L, table, checkpoints=(10, 40, 160, 640), batch
     return out
 
 
+# Exact counts of the 9 categories over all 133,784,560 seven-card hands, and
+# the first rank of each category on the 1..7462 scale.
+SEVEN_CARD_CATEGORIES = [23294460, 58627800, 31433400, 6461620, 6180020, 4047644, 3473184, 224848, 41584]
+CATEGORY_START = [1, 1278, 4138, 4996, 5854, 5864, 7141, 7297, 7453, 7463]
+
+
+def c4_showdown(m, L, table, total=1 << 28, chunk=1 << 24) -> dict:
+    """Showdown microbench: `total` uniform 7-card hands (seeded, without
+    replacement within a hand) evaluated on the device by mccfr_eval7_device,
+    timed with its CUDA events; 7 dependent rank-table gathers (28 B) per hand.
+    The category frequencies are checked against the exact counts."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    t = m.GPUCFRTrainer(config=L.preset(L.PRESET_HU_20BB), table_log2=10)
+    t.set_hand_table(table)
+    lib = L.load()
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(3)
+    ranks = torch.empty(chunk, dtype=torch.int16, device="cuda")
+    hist = torch.zeros(7463, dtype=torch.int64, device="cuda")
+    ms_total = 0.0
+    for _ in range(total // chunk):
+        cards = torch.rand(chunk, 52, device="cuda", generator=gen).argsort(dim=1)[:, :7].to(torch.uint8).contiguous()
+        ms = ctypes.c_float()
+        L.check(lib.mccfr_eval7_device(t.handle, ctypes.c_void_p(cards.data_ptr()), ctypes.c_void_p(ranks.data_ptr()),
+                                       chunk, ctypes.byref(ms)))
+        ms_total += ms.value
+        hist += torch.bincount(ranks.to(torch.int64) & 0xFFFF, minlength=7463)[:7463]
+        del cards
+    t.close()
+    h = hist.cpu().numpy()
+    n = (total // chunk) * chunk
+    obs = np.array([h[CATEGORY_START[i]:CATEGORY_START[i + 1]].sum() for i in range(9)], dtype=np.float64)
+    p = np.array(SEVEN_CARD_CATEGORIES, dtype=np.float64) / 133784560.0
+    z = (obs / n - p) / np.sqrt(p * (1 - p) / n)
+    evals = n / (ms_total / 1e3)
+    peak, kind = measured_peak()
+    return {"hands": n, "hand_evals_per_s": evals, "kernel_ms": ms_total,
+            "gather_gbs": 28.0 * evals / 1e9, "gather_frac_of_hbm_peak": 28.0 * evals / 1e9 / peak,
+            "category_max_abs_z": float(np.abs(z).max()), "invalid_ranks": int(h[0]),
+            "workload": "2^28 uniform 7-card hands in chunks of 2^24 (torch generator seed 3, cards on the "
+                        "device), k_eval7: one thread per hand, 7 dependent gathers into the 130 MB rank table"}
+
+
 def hu_full_exploitability(m, L, table, iters: int, stride: int) -> dict:
     """Heads-up 20BB from the blinds: both update rules trained for `iters`
     iterations of 65,536 traversals per player-update, then the exact best
@@ -523,6 +570,7 @@ def main():
                      "algorithmic_bytes": "40*V + 96*U per launch (V node visits, U updating-player updates)",
                      "V_per_traversal": visits / max(1, trav), "U_per_traversal": updates / max(1, trav)},
         "node_visits_per_s": visits / (ms / 1e3) * world,
+        "hand_evals_per_s": (s1.hand_evals - s0.hand_evals) / (ms / 1e3) * world,
     }
 
     tr.close()
@@ -532,6 +580,7 @@ def main():
         extras["c3_multitable"] = multitable(m, L, table)
         extras["resolve_serving"] = serving_sweep(m, L, table)
         extras["hu_subgame_exploitability"] = hu_subgame_exploitability(m, L, table)
+        extras["c4_showdown"] = c4_showdown(m, L, table)
         for wl in ("ref8-6max", "6max-100bb-refrule"):
             if wl == args.workload:
                 continue
