@@ -386,6 +386,7 @@ def c4_showdown(m, L, table, total=1 << 28, chunk=1 << 24) -> dict:
     ms_total = 0.0
     for _ in range(total // chunk):
         cards = torch.rand(chunk, 52, device="cuda", generator=gen).argsort(dim=1)[:, :7].to(torch.uint8).contiguous()
+        torch.cuda.synchronize()  # the library evaluates on its own stream
         ms = ctypes.c_float()
         L.check(lib.mccfr_eval7_device(t.handle, ctypes.c_void_p(cards.data_ptr()), ctypes.c_void_p(ranks.data_ptr()),
                                        chunk, ctypes.byref(ms)))
