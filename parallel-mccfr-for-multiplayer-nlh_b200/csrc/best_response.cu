@@ -5,7 +5,7 @@
 // expensive).  This engine evaluates an average strategy, given as info-set
 // rows (key, strategy sum), in the game the traversal kernels play:
 //   * the public tree is built by the kernels' own rules (valid_mask,
-//     chips_for, the raise cap, the action queue and depth cut of es_walk in
+//     chips_for, the raise cap, the action queue and depth cut of es_step in
 //     traverse_es.cuh; es_apply's bookkeeping) and keys by info_key, so a node
 //     here is an info-set row there;
 //   * the walk is vector-valued: at each public state it carries both players'
@@ -135,7 +135,7 @@ struct Node {
   long long strat = -1;  // full game: offset of the node's dense strategy table
 };
 
-// Betting state of es_walk (traverse_es.cuh), two players.
+// Betting state of the traversal walk (EsState, traverse_es.cuh), two players.
 struct St {
   int stack[2], bet[2], inv[2];
   int pot, cb, lfr;
@@ -181,7 +181,7 @@ void apply_action(const GameParams& G, St& s, int player, int a) {
   }
 }
 
-// Public tree from state s, in es_walk's order of checks: depth cut, one
+// Public tree from state s, in es_step's order of checks: depth cut, one
 // player left, end of the street's queue (deal or showdown), decision.
 int build_tree(const GameParams& G, std::vector<Node>& T, St s, int dealer) {
   auto push = [&](const Node& n) {

@@ -340,16 +340,6 @@ __device__ __forceinline__ int es_step(const GameParams& G, const TableView& tv,
   return 0;
 }
 
-// One whole traversal (the batched kernel's unit of work).
-template <int W, class Frames>
-__device__ __forceinline__ void es_walk(const GameParams& G, const TableView& tv, const DealRec* D, uint32_t t,
-                                        uint32_t uid, int up, float rscale, Frames& fr, EsCounts& cnt) {
-  EsLane L;
-  es_begin(G, D, t, L);
-  while (es_step<W>(G, tv, uid, up, rscale, fr, L, cnt) == 0) {
-  }
-}
-
 // Persistent traversal kernel: every lane takes its next traversal from the
 // device work counter as soon as its current one is complete (lanes that need
 // work together share one atomic), inside the same one-event-per-iteration
