@@ -70,6 +70,23 @@ def make_config(L, workload: str, rank: int = 0):
     return cfg, batch
 
 
+def over_ranks(ms: float, traversals: int, e2e_s: float, device) -> tuple[float, float, float]:
+    """Whole-job figures from one replica's own: the slowest rank's device time
+    and end-to-end wall time (MAX) and the traversals of all ranks (SUM).  With one
+    rank, or no process group, a rank's own figures come back unchanged; several
+    ranks all take the same two all-reduces in the same order."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(ms), float(traversals), float(e2e_s)
+    t = torch.tensor([ms, e2e_s], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    n = torch.tensor([float(traversals)], dtype=torch.float64, device=device)
+    dist.all_reduce(n, op=dist.ReduceOp.SUM)
+    return float(t[0].item()), float(n[0].item()), float(t[1].item())
+
+
 def describe(cfg, workload, batch) -> dict:
     kinds = {0: "fold", 1: "check", 2: "call", 3: "check/call", 4: "min-raise", 6: "all-in"}
     acts = []
@@ -519,16 +536,6 @@ def main():
     updates = s1.traverser_updates - s0.traverser_updates
     launches = args.steps * cfg.num_players
     trav_ms = s1.traverse_ms - s0.traverse_ms
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-        n = torch.tensor([trav], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(n, op=dist.ReduceOp.SUM)
-        total = float(n.item())
-    else:
-        ms_max, total = ms, float(trav)
-    value = total / (ms_max / 1e3)
 
     # e2e through the C ABI: host call per step, schedule H2D inside, stats D2H read
     t0 = time.perf_counter()
@@ -537,13 +544,10 @@ def main():
         tr.train(1, batch, verbose=False)
         st = tr.stats()
     e2e_s = time.perf_counter() - t0
-    e2e_local = e2e_steps * batch * cfg.num_players / e2e_s
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_value = world * e2e_steps * batch * cfg.num_players / float(t.item())
-    else:
-        e2e_value = e2e_local
+
+    ms_max, total, e2e_s_max = over_ranks(ms, trav, e2e_s, f"cuda:{local_rank}")
+    value = total / (ms_max / 1e3)
+    e2e_value = world * e2e_steps * batch * cfg.num_players / e2e_s_max
 
     peak, peak_kind = measured_peak()
     bytes_per_launch = (40.0 * visits + 96.0 * updates) / launches
