@@ -70,6 +70,16 @@ def make_config(L, workload: str, rank: int = 0):
     return cfg, batch
 
 
+def apply_roofline(s0, s1, launches: int, peak: float) -> dict:
+    """The apply kernel's share of a step against the HBM roofline: 516 B per touched
+    row (the 256-byte record read and written, the list entry read)."""
+    ms = (s1.apply_ms - s0.apply_ms) / max(1, launches)
+    rows = int(s1.touched_last)
+    gbs = rows * 516.0 / (ms / 1e3) / 1e9 if ms > 0 else None
+    return {"kernel": "k_apply", "kernel_ms_per_launch": ms, "touched_rows_last_update": rows,
+            "bytes_per_row": 516, "achieved": gbs, "unit": "GB/s", "frac": gbs / peak if gbs else None}
+
+
 def over_ranks(ms: float, traversals: int, e2e_s: float, device) -> tuple[float, float, float]:
     """Whole-job figures from one replica's own: the slowest rank's device time
     and end-to-end wall time (MAX) and the traversals of all ranks (SUM).  With one
@@ -550,6 +560,7 @@ def main():
     e2e_value = world * e2e_steps * batch * cfg.num_players / e2e_s_max
 
     peak, peak_kind = measured_peak()
+    rows_used = tr.rows_used()
     bytes_per_launch = (40.0 * visits + 96.0 * updates) / launches
     kernel_ms = trav_ms / launches if trav_ms > 0 else None
     achieved = bytes_per_launch / (kernel_ms / 1e3) / 1e9 if kernel_ms else None
@@ -574,6 +585,12 @@ def main():
                      "kernel_ms_per_launch": kernel_ms,
                      "algorithmic_bytes": "40*V + 96*U per launch (V node visits, U updating-player updates)",
                      "V_per_traversal": visits / max(1, trav), "U_per_traversal": updates / max(1, trav)},
+        # k_apply folds each touched row: both 128-byte lines of its record read and written, plus
+        # its 4-byte touched-list entry; rows counted on the device for the last player-update
+        "apply": apply_roofline(s0, s1, launches, peak),
+        "table": {"rows_used": rows_used, "capacity": int(s1.table_capacity),
+                  "load": rows_used / max(1, s1.table_capacity), "record_bytes": 256,
+                  "span_gb": s1.table_capacity * 256 / 1e9},
         "node_visits_per_s": visits / (ms / 1e3) * world,
         "hand_evals_per_s": (s1.hand_evals - s0.hand_evals) / (ms / 1e3) * world,
     }

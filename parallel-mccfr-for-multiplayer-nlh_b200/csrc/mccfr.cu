@@ -393,6 +393,14 @@ int validate(const mccfr_config& c, std::string& why) {
   return 0;
 }
 
+// Every key lies in [1, 2^kb]: an FNV26 key is a 26-bit slot plus one, an ID64
+// key reduced to key_bits bits is that plus one.  When 2^kb is below the
+// capacity, key k owns row k and the table needs no probing.
+int direct_map(const mccfr_config& c) {
+  const int kb = c.key_mode == MCCFR_KEY_FNV26 ? 26 : c.key_bits;
+  return kb > 0 && kb < c.table_log2 ? 1 : 0;
+}
+
 void make_params(const mccfr_config& c, GameParams& g) {
   std::memset(&g, 0, sizeof(g));
   g.N = c.num_players;
@@ -849,6 +857,7 @@ int mccfr_create(const mccfr_config* cfg, mccfr_handle** out) {
   h->tv.err = reinterpret_cast<int*>(misc + 64);
   h->tv.mask = C - 1;
   h->tv.log2cap = cfg->table_log2;
+  h->tv.direct = direct_map(*cfg);
   *out = h;
   return MCCFR_OK;
 #undef CKC
@@ -1028,6 +1037,13 @@ int mccfr_train(mccfr_handle* h, long long iters, int batch, int verbose, const 
         h->apply_ms += t2;
         h->last_traverse_ms = t1;
         h->last_apply_ms = t2;
+      }
+      if (i + 1 == iters) {
+        // rows touched by this iteration's last player-update (its parity's counter
+        // is reset only by the next update's apply)
+        unsigned nt[2] = {0, 0};
+        CK(cudaMemcpy(nt, h->tv.n_touched, sizeof(nt), cudaMemcpyDeviceToHost));
+        h->touched_last = nt[(uint32_t)((h->iterations_done + i) * np + np - 1) & 1];
       }
     }
     h->launches += h->cfg.num_players;
@@ -1816,6 +1832,7 @@ int mccfr_subgame_reset(mccfr_handle* h, const mccfr_config* cfg, const mccfr_su
   CK(cudaMemsetAsync(h->d_counters, 0, sizeof(Counters), h->stream));
   CK(cudaStreamSynchronize(h->stream));
   h->cfg = *cfg;
+  h->tv.direct = direct_map(*cfg);
   make_params(*cfg, h->gp);
   set_subgame_params(h, cfg, sg, nb);
   if (h->graph) {

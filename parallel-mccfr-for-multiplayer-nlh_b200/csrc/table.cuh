@@ -4,7 +4,8 @@
 // 1106-1136).  Each row is one 256-byte record (two 128-byte lines), so that a
 // visit touches two adjacent sectors and folding a row in reads one contiguous
 // record instead of a dozen scattered ones:
-//     0  key    u64   0 = empty; linear probing from the key's home slot
+//     0  key    u64   0 = empty; linear probing from the key's home slot, or row k
+//                       for key k when every key is below the capacity (direct map)
 //     8  tag    u64   ((update id + 1) << 8) | canonical action mask of that update
 //    16  cnt    u64   (all visits << 32) | visits whose mask is the canonical one
 //    24  su     i64   sum of fix(u) (reference rule) or fix(v_h) (external sampling)
@@ -30,6 +31,7 @@ struct TableView {
   unsigned int* n_touched;   // [2], indexed by update-id parity
   unsigned long long mask;   // cap - 1
   int log2cap;
+  int direct;                // every key is below cap: key k owns row k, no probing
   int* err;
 };
 
@@ -80,9 +82,11 @@ __device__ __forceinline__ unsigned long long home_slot(const TableView& tv, uns
 }
 
 // Read-only lookup; returns the slot or -1.  W keys are loaded per probe step
-// (independent loads issued together); W is an autotuned probe width.
+// (independent loads issued together); W is an autotuned probe width.  A
+// direct-mapped table reads the key's own row only.
 template <int W = 1>
 __device__ __forceinline__ long long table_find(const TableView& tv, unsigned long long key) {
+  if (tv.direct) return __ldcg(row_key(tv, key)) == key ? (long long)key : -1ll;
   unsigned long long s = home_slot(tv, key);
   for (int step = 0; step < kProbeLimit; step += W) {
     unsigned long long k[W];
@@ -99,8 +103,15 @@ __device__ __forceinline__ long long table_find(const TableView& tv, unsigned lo
 }
 
 // Find or insert; returns the slot, or -1 when the probe limit is exceeded.
+// In a direct-mapped table row k can hold no key but k, so every writer of the
+// key stores the same value and no atomic is needed.
 template <int W = 1>
 __device__ __forceinline__ long long table_insert(const TableView& tv, unsigned long long key) {
+  if (tv.direct) {
+    unsigned long long* kp = row_key(tv, key);
+    if (__ldcg(kp) != key) __stcg(kp, key);
+    return (long long)key;
+  }
   unsigned long long s = home_slot(tv, key);
   for (int step = 0; step < kProbeLimit; step += W) {
     unsigned long long k[W];

@@ -165,6 +165,15 @@ class GPUCFRTrainer:
         L.check(self._lib.mccfr_get_strategy(self._h, L.ptr(keys), None, L.ptr(probs), cap, byref(n)), self._h)
         return keys[: n.value], probs[: n.value]
 
+    def rows_used(self) -> int:
+        """Occupied rows of the info-set table, counted on the device (the
+        size query of mccfr_export_rows: capacity 0, no copy)."""
+        n = c_size_t()
+        rc = self._lib.mccfr_export_rows(self._h, None, None, None, None, 0, byref(n))
+        if rc not in (L.OK, L.ERR_CAPACITY):
+            L.check(rc, self._h)
+        return int(n.value)
+
     def export_rows(self) -> dict[str, np.ndarray]:
         n = c_size_t()
         rc = self._lib.mccfr_export_rows(self._h, None, None, None, None, 0, byref(n))

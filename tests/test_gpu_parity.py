@@ -94,6 +94,34 @@ def test_external_sampling_on_reference_game(hand_table):
     assert_rows_equal(tr.export_rows(), orc.export_rows())
 
 
+@pytest.mark.parametrize("preset,sampling,batch", [
+    (L.PRESET_6MAX_100BB, L.SAMPLING_EXTERNAL, 64),
+    (L.PRESET_HU_20BB, L.SAMPLING_EXTERNAL, 2048),
+    (L.PRESET_HU_20BB, L.SAMPLING_REFERENCE, 2048),
+])
+def test_direct_mapped_table_bit_exact(hand_table, preset, sampling, batch):
+    """Keys reduced to 20 bits: in a 2^21-row table key k owns row k and no
+    lookup probes; a 2^20-row table holding the same keys probes.  Both equal
+    the oracle bit for bit."""
+    over = dict(key_bits=20, sampling=sampling)
+    if sampling == L.SAMPLING_REFERENCE:
+        over["max_depth"] = 64
+    cfg, direct, orc = make_pair(preset, hand_table, table_log2=21, **over)
+    cfg.table_log2 = 20
+    probed = mccfr.GPUCFRTrainer(config=cfg)
+    probed.set_hand_table(hand_table)
+    for it in (1, 2):
+        for p in range(cfg.num_players):
+            direct.step(it, p, batch)
+            probed.step(it, p, batch)
+            orc.step(it, p, batch)
+    want = orc.export_rows()
+    assert_rows_equal(direct.export_rows(), want)
+    assert_rows_equal(probed.export_rows(), want)
+    assert want["keys"].size < (1 << 19)  # the probed table stayed under half full
+    assert want["keys"].max() <= (1 << 20)
+
+
 def test_graph_training_equals_steps(hand_table):
     cfg = L.preset(L.PRESET_REF8)
     cfg.table_log2 = 20
@@ -101,11 +129,17 @@ def test_graph_training_equals_steps(hand_table):
     b = mccfr.GPUCFRTrainer(config=cfg)
     a.set_hand_table(hand_table)
     b.set_hand_table(hand_table)
-    a.train(3, 2048, verbose=False)
+    a.train(2, 2048, verbose=False)
+    a.train(1, 2048, verbose=False, timed=True)
     for it in (1, 2, 3):
         for p in range(2):
             b.step(it, p, 2048)
     assert_rows_equal(a.export_rows(), b.export_rows())
+    # the timed graph path counts the last update's touched rows like a step does
+    sa, sb = a.stats(), b.stats()
+    assert sa.touched_last == sb.touched_last > 0
+    assert sa.apply_ms > 0.0
+    assert a.rows_used() == b.export_rows()["keys"].size >= sa.touched_last
 
 
 def test_fp32_reference_order_within_tolerance(hand_table):
