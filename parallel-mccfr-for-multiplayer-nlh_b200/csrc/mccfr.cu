@@ -394,11 +394,11 @@ int validate(const mccfr_config& c, std::string& why) {
 }
 
 // Every key lies in [1, 2^kb]: an FNV26 key is a 26-bit slot plus one, an ID64
-// key reduced to key_bits bits is that plus one.  When 2^kb is below the
-// capacity, key k owns row k and the table needs no probing.
+// key reduced to key_bits bits is that plus one.  When 2^kb rows fit in the
+// table, key k owns row k-1 and the table needs no probing.
 int direct_map(const mccfr_config& c) {
   const int kb = c.key_mode == MCCFR_KEY_FNV26 ? 26 : c.key_bits;
-  return kb > 0 && kb < c.table_log2 ? 1 : 0;
+  return kb > 0 && kb <= c.table_log2 ? 1 : 0;
 }
 
 void make_params(const mccfr_config& c, GameParams& g) {

@@ -4,8 +4,8 @@
 // 1106-1136).  Each row is one 256-byte record (two 128-byte lines), so that a
 // visit touches two adjacent sectors and folding a row in reads one contiguous
 // record instead of a dozen scattered ones:
-//     0  key    u64   0 = empty; linear probing from the key's home slot, or row k
-//                       for key k when every key is below the capacity (direct map)
+//     0  key    u64   0 = empty; linear probing from the key's home slot, or row k-1
+//                       for key k when every key is at most the capacity (direct map)
 //     8  tag    u64   ((update id + 1) << 8) | canonical action mask of that update
 //    16  cnt    u64   (all visits << 32) | visits whose mask is the canonical one
 //    24  su     i64   sum of fix(u) (reference rule) or fix(v_h) (external sampling)
@@ -31,7 +31,7 @@ struct TableView {
   unsigned int* n_touched;   // [2], indexed by update-id parity
   unsigned long long mask;   // cap - 1
   int log2cap;
-  int direct;                // every key is below cap: key k owns row k, no probing
+  int direct;                // every key is at most cap: key k owns row k-1, no probing
   int* err;
 };
 
@@ -86,7 +86,7 @@ __device__ __forceinline__ unsigned long long home_slot(const TableView& tv, uns
 // direct-mapped table reads the key's own row only.
 template <int W = 1>
 __device__ __forceinline__ long long table_find(const TableView& tv, unsigned long long key) {
-  if (tv.direct) return __ldcg(row_key(tv, key)) == key ? (long long)key : -1ll;
+  if (tv.direct) return __ldcg(row_key(tv, key - 1)) == key ? (long long)(key - 1) : -1ll;
   unsigned long long s = home_slot(tv, key);
   for (int step = 0; step < kProbeLimit; step += W) {
     unsigned long long k[W];
@@ -103,14 +103,14 @@ __device__ __forceinline__ long long table_find(const TableView& tv, unsigned lo
 }
 
 // Find or insert; returns the slot, or -1 when the probe limit is exceeded.
-// In a direct-mapped table row k can hold no key but k, so every writer of the
-// key stores the same value and no atomic is needed.
+// In a direct-mapped table row k-1 can hold no key but k, so every writer of
+// the key stores the same value and no atomic is needed.
 template <int W = 1>
 __device__ __forceinline__ long long table_insert(const TableView& tv, unsigned long long key) {
   if (tv.direct) {
-    unsigned long long* kp = row_key(tv, key);
+    unsigned long long* kp = row_key(tv, key - 1);
     if (__ldcg(kp) != key) __stcg(kp, key);
-    return (long long)key;
+    return (long long)(key - 1);
   }
   unsigned long long s = home_slot(tv, key);
   for (int step = 0; step < kProbeLimit; step += W) {

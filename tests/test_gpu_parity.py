@@ -100,10 +100,10 @@ def test_external_sampling_on_reference_game(hand_table):
     (L.PRESET_HU_20BB, L.SAMPLING_REFERENCE, 2048),
 ])
 def test_direct_mapped_table_bit_exact(hand_table, preset, sampling, batch):
-    """Keys reduced to 20 bits: in a 2^21-row table key k owns row k and no
+    """Keys reduced to 21 bits: in a 2^21-row table key k owns row k-1 and no
     lookup probes; a 2^20-row table holding the same keys probes.  Both equal
     the oracle bit for bit."""
-    over = dict(key_bits=20, sampling=sampling)
+    over = dict(key_bits=21, sampling=sampling)
     if sampling == L.SAMPLING_REFERENCE:
         over["max_depth"] = 64
     cfg, direct, orc = make_pair(preset, hand_table, table_log2=21, **over)
@@ -118,8 +118,8 @@ def test_direct_mapped_table_bit_exact(hand_table, preset, sampling, batch):
     want = orc.export_rows()
     assert_rows_equal(direct.export_rows(), want)
     assert_rows_equal(probed.export_rows(), want)
-    assert want["keys"].size < (1 << 19)  # the probed table stayed under half full
-    assert want["keys"].max() <= (1 << 20)
+    assert want["keys"].size < (1 << 20)  # every key fit the probed table (6-max: 56% full)
+    assert want["keys"].max() <= (1 << 21)
 
 
 def test_graph_training_equals_steps(hand_table):
