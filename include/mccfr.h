@@ -109,7 +109,10 @@ typedef struct mccfr_config {
   uint64_t seed;            /* Philox key */
   /* ID64 keys only: when > 0, keys are reduced to key_bits bits (plus one), so
      at most 2^key_bits rows exist and identities that share the reduced key share
-     a row, as the reference's 2^26 direct-mapped slots do.  0 = full 64 bits. */
+     a row, as the reference's 2^26 direct-mapped slots do.  0 = full 64 bits.
+     When every key fits the table (key_bits <= table_log2; for FNV26 keys,
+     table_log2 >= 26), key k owns row k-1 and lookups never probe; otherwise
+     the table is open-addressed.  Results are the same either way. */
   int32_t key_bits;
   int32_t reserved[7];
 } mccfr_config;
