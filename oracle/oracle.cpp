@@ -1216,6 +1216,47 @@ void orc_rank_hist(const int32_t* T, int ncards, uint64_t* out) {
   std::memcpy(out, c.data(), 7463 * sizeof(uint64_t));
 }
 
+// Order-sensitive digests of the 7-card ranks of all C(52, 7) hands, grouped
+// by their two lowest cards (a, b).  Within a group the hands {a < b < c < d <
+// e < f < g} run in lexicographic order with i = 0, 1, ...; the digests are
+// sum[a*52+b] = sum of ranks and wsum[a*52+b] = sum of (i+1) * rank.  The
+// chains share prefixes as in rank_hist (cfr_gpu.cu:114-150).
+void orc_rank7_digests(const int32_t* T, uint64_t* sum, uint64_t* wsum) {
+  std::memset(sum, 0, 52 * 52 * sizeof(uint64_t));
+  std::memset(wsum, 0, 52 * 52 * sizeof(uint64_t));
+  std::vector<std::thread> th;
+  for (int t = 0; t < 8; ++t)
+    th.emplace_back([=] {
+      for (int a = t; a < 52; a += 8) {
+        const int32_t pa = T[53 + to_rm(a)];
+        for (int b = a + 1; b < 52; ++b) {
+          const int32_t pb = T[pa + to_rm(b)];
+          uint64_t s = 0, w = 0, i = 0;
+          for (int c = b + 1; c < 52; ++c) {
+            const int32_t pc = T[pb + to_rm(c)];
+            for (int d = c + 1; d < 52; ++d) {
+              const int32_t pd = T[pc + to_rm(d)];
+              for (int e = d + 1; e < 52; ++e) {
+                const int32_t pe = T[pd + to_rm(e)];
+                for (int f = e + 1; f < 52; ++f) {
+                  const int32_t pf = T[pe + to_rm(f)];
+                  for (int g = f + 1; g < 52; ++g) {
+                    const uint64_t r = decode16((uint16_t)T[pf + to_rm(g)]);
+                    s += r;
+                    w += ++i * r;
+                  }
+                }
+              }
+            }
+          }
+          sum[a * 52 + b] = s;
+          wsum[a * 52 + b] = w;
+        }
+      }
+    });
+  for (auto& x : th) x.join();
+}
+
 // Rank after chaining n cards (0..51) through the table in the given order; for
 // n = 5 or 6 the chain ends on a state, whose card-0 entry holds the hand's rank.
 int orc_chain_rank(const int32_t* T, const uint8_t* cards, int n) {

@@ -168,6 +168,55 @@ def test_eval7_matches_oracle(hand_table):
     assert np.array_equal(tr.eval7(cards), binding.eval7(hand_table, cards))
 
 
+def test_eval7_exhaustive_sweep(hand_table):
+    """All C(52, 7) = 133,784,560 hands ranked on the device (mccfr_eval7_device),
+    in lexicographic order grouped by the two lowest cards (a, b): each group's
+    sum and position-weighted sum of ranks equal the oracle's, so no hand of the
+    sweep is missing, misranked or out of order."""
+    import ctypes
+    import itertools
+
+    import torch
+
+    cfg = L.preset(L.PRESET_REF8)
+    cfg.table_log2 = 12
+    tr = mccfr.GPUCFRTrainer(config=cfg)
+    tr.set_hand_table(hand_table)
+    lib = L.load()
+    want_s = np.zeros(52 * 52, np.uint64)
+    want_w = np.zeros(52 * 52, np.uint64)
+    binding.lib().orc_rank7_digests(binding._p(hand_table), binding._p(want_s), binding._p(want_w))
+    dev = torch.device("cuda:0")
+    # the 5-card completions: combinations of 0..49 in lexicographic order; those
+    # below m, shifted by b + 1, are the completions of cards above b
+    c5 = torch.from_numpy(np.array(list(itertools.combinations(range(50), 5)), np.uint8)).to(dev)
+    got_s = torch.zeros(52 * 52, dtype=torch.int64, device=dev)
+    got_w = torch.zeros(52 * 52, dtype=torch.int64, device=dev)
+    hands = 0
+    for b in range(1, 47):
+        tail = c5[c5[:, 4] < 51 - b] + (b + 1)  # cards b+1 .. 51
+        n = tail.shape[0]
+        pos = torch.arange(1, n + 1, dtype=torch.int64, device=dev)
+        cards = torch.empty((n, 7), dtype=torch.uint8, device=dev)
+        cards[:, 2:] = tail
+        ranks = torch.empty(n, dtype=torch.int16, device=dev)
+        for a in range(b):
+            cards[:, 0] = a
+            cards[:, 1] = b
+            torch.cuda.synchronize()  # the library evaluates on its own stream
+            L.check(lib.mccfr_eval7_device(tr.handle, ctypes.c_void_p(cards.data_ptr()),
+                                           ctypes.c_void_p(ranks.data_ptr()), n, None))
+            r = ranks.to(torch.int64) & 0xFFFF
+            got_s[a * 52 + b] = r.sum()
+            got_w[a * 52 + b] = (r * pos).sum()
+            hands += n
+    torch.cuda.synchronize()
+    assert hands == 133784560
+    assert np.array_equal(got_s.cpu().numpy().astype(np.uint64), want_s)
+    assert np.array_equal(got_w.cpu().numpy().astype(np.uint64), want_w)
+    tr.close()
+
+
 def test_checkpoint_and_dump_roundtrip(hand_table, tmp_path):
     cfg = L.preset(L.PRESET_REF8)
     cfg.table_log2 = 20

@@ -70,6 +70,24 @@ def test_exhaustive_category_counts(hand_table):
     assert np.count_nonzero(h5[1:]) == 7462
 
 
+def test_rank7_digests(hand_table):
+    """The oracle's per-group digests of the exhaustive 7-card sweep (the GPU
+    sweep's checker): their sums agree with the exhaustive histogram, and two
+    groups agree with per-hand ranks in lexicographic order."""
+    s = np.zeros(52 * 52, np.uint64)
+    w = np.zeros(52 * 52, np.uint64)
+    binding.lib().orc_rank7_digests(binding._p(hand_table), binding._p(s), binding._p(w))
+    h7 = binding.rank_hist(hand_table, 7)
+    assert int(s.sum()) == int((h7 * np.arange(7463, dtype=np.uint64)).sum())
+    assert np.count_nonzero(s) == sum(b for b in range(1, 47))  # groups with 5 cards above b
+    for a, b in ((0, 1), (30, 44)):
+        tails = np.array(list(itertools.combinations(range(b + 1, 52), 5)), np.uint8)
+        cards = np.concatenate([np.full((len(tails), 2), (a, b), np.uint8), tails], axis=1)
+        r = binding.eval7(hand_table, cards).astype(np.uint64)
+        assert int(r.sum()) == int(s[a * 52 + b])
+        assert int((r * np.arange(1, len(r) + 1, dtype=np.uint64)).sum()) == int(w[a * 52 + b])
+
+
 def test_against_brute_force(hand_table):
     rng = np.random.default_rng(7)
     cards = np.stack([rng.permutation(52)[:7] for _ in range(200000)]).astype(np.uint8)
