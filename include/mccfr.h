@@ -126,7 +126,8 @@ typedef struct mccfr_stats {
   int64_t traverser_updates; /* updating-player nodes updated (U) */
   int64_t terminals;         /* terminal values computed */
   int64_t hand_evals;        /* rank-chain evaluations */
-  int64_t rows_used;         /* occupied info-set rows */
+  int64_t rows_used;         /* -1 here: counting takes a table pass; the size query of
+                                mccfr_export_rows (capacity 0) returns the occupied rows */
   int64_t table_capacity;
   int64_t touched_last;      /* rows touched by the last player-update */
   double traverse_ms;        /* summed CUDA-event time of traversal kernels */
@@ -241,7 +242,7 @@ int mccfr_eval7_device(mccfr_handle* h, const uint8_t* dev_cards,
                        uint16_t* dev_ranks, size_t n, float* ms);
 
 /* ---- batched form: many tables in one persistent kernel ------------------
-   No reference counterpart (SURVEY N1).  A batch groups existing handles
+   No reference counterpart.  A batch groups existing handles
    (tables), each with its own game, table and schedule; one iteration runs
    phase p = 0..max players-1 as ONE persistent traversal launch over the
    player-p updates of every table with more than p players, pulling
@@ -286,7 +287,7 @@ int mccfr_batch_autotune(mccfr_batch* b, int max_candidates, mccfr_batch_tuning*
 int mccfr_batch_get_stats(mccfr_batch* b, mccfr_batch_stats* out);
 
 /* ---- subgame re-solve and continuous batching -----------------------------
-   No reference counterpart (SURVEY N2).  A subgame starts on the turn or the
+   No reference counterpart.  A subgame starts on the turn or the
    river with a known board, a dead pot shared equally by the players, equal
    stacks (cfg->starting_stack), and one 1326-combo range per player (combo of
    cards lo < hi is index hi*(hi-1)/2 + lo; combos that use a board card get
@@ -339,7 +340,7 @@ int mccfr_eval7_static(const int32_t* dev_table, const uint8_t* cards, uint16_t*
 
 /* ---- heads-up best response and exploitability -------------------------
    No counterpart in the reference (its PROPOSAL.md:99 calls exploitability too
-   expensive; play is judged against scripted bots).  An exact best response
+   expensive; play is measured against scripted bots).  An exact best response
    in double precision on host threads, for heads-up games only: the full game
    from the blinds (rank-CDF postflop buckets, which are suit-invariant, so
    flops are enumerated up to suit permutation), or a turn/river subgame.  The

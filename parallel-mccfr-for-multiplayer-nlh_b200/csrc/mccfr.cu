@@ -1327,7 +1327,7 @@ int mccfr_eval7(mccfr_handle* h, const uint8_t* cards, uint16_t* ranks, size_t n
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
-// Batched form (SURVEY N1): many tables in one persistent kernel.
+// Batched form: many tables in one persistent kernel.
 // ---------------------------------------------------------------------------
 struct mccfr_batch {
   std::vector<mccfr_handle*> tables;
@@ -1694,7 +1694,7 @@ int mccfr_batch_get_stats(mccfr_batch* b, mccfr_batch_stats* out) {
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
-// Subgames and continuous batching (SURVEY N2).
+// Subgames and continuous batching.
 // ---------------------------------------------------------------------------
 namespace {
 
