@@ -183,8 +183,16 @@ def profiled_traffic(workload: str) -> dict | None:
         return None
 
 
-def cpu_traversal_rate(L, cfg, batch_sample: int, reps: int = 1) -> tuple[float, dict]:
-    """The oracle (the reference path's C++ restatement) on host cores."""
+def cpu_traversal_rate(L, cfg, batch_sample: int, visits_per_traversal: float | None = None) -> tuple[float, dict]:
+    """The oracle (the reference path's C++ restatement) on host cores, timed on
+    one player-update of `batch_sample` traversals from an empty table.
+
+    A traversal's cost depends on the training state: from an empty table every
+    strategy is uniform and a 6-max traversal visits about 1,000 decision nodes,
+    where the GPU's timed iterations visit about 55.  Given the node visits per
+    traversal of the iterations being compared, the rate is returned in
+    traversals of that size: the oracle's node visits per second divided by it.
+    The raw figures stay in the info dict."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import binding
 
@@ -192,12 +200,34 @@ def cpu_traversal_rate(L, cfg, batch_sample: int, reps: int = 1) -> tuple[float,
     table = L.hand_table()
     orc = binding.Oracle(cfg, table)
     t0 = time.perf_counter()
-    it = 1
-    for r in range(reps):
-        orc.step(it, r % cfg.num_players, batch_sample, threads=threads)
+    orc.step(1, 0, batch_sample, threads=threads)
     dt = time.perf_counter() - t0
+    visits = orc.counters()["visits"]
     orc.close()
-    return batch_sample * reps / dt, {"cores": threads, "seconds": dt}
+    info = {"cores": threads, "seconds": dt, "raw_traversals_per_s": batch_sample / dt,
+            "visits_per_traversal": visits / batch_sample, "visits_per_s": visits / dt}
+    if visits_per_traversal:
+        return visits / dt / visits_per_traversal, info
+    return batch_sample / dt, info
+
+
+def work_per_traversal(workload: str) -> float | None:
+    """Decision-node visits per traversal of the bench's timed iterations on this
+    workload, measured on the GPU (profiles/work_per_traversal.json)."""
+    try:
+        d = json.loads((ROOT / "profiles" / "work_per_traversal.json").read_text())
+        return float(d[workload]["visits_per_traversal"])
+    except Exception:
+        return None
+
+
+def cpu_sample_text(sample: int, info: dict, v: float | None) -> str:
+    head = (f"{sample} traversals of one player-update from an empty table (iteration 1, player 0), "
+            f"{info['seconds']:.1f} s on {info['cores']} threads: {info['visits_per_traversal']:.0f} node visits "
+            f"per traversal, {info['visits_per_s']:.3g} visits/s, {info['raw_traversals_per_s']:.0f} raw traversals/s")
+    if v:
+        return head + f"; value = visits/s / {v:.2f} visits per traversal of the GPU's timed iterations"
+    return head + "; value = raw traversals/s (no GPU visit count recorded for this workload)"
 
 
 def batched_same_table(m, L, table, args, plain_value) -> dict:
@@ -484,17 +514,19 @@ def main():
             return
         # bounded per-step samples of the same workload on all host cores
         sample = {"6max-100bb": 1024, "6max-100bb-refrule": 16384, "hu-20bb": 8192}.get(args.workload, 65536)
+        vpt = work_per_traversal(args.workload)
         for _ in range(args.warmup):
-            cpu_traversal_rate(L, cfg, max(64, sample // 8))
+            cpu_traversal_rate(L, cfg, max(64, sample // 8), vpt)
         rates, secs = [], 0.0
         cores = os.cpu_count() or 1
+        info = {}
         for _ in range(args.steps):
-            r, info = cpu_traversal_rate(L, cfg, sample)
+            r, info = cpu_traversal_rate(L, cfg, sample, vpt)
             rates.append(r)
             secs += info["seconds"]
             cores = info["cores"]
         v = statistics.median(rates)
-        desc = f"{sample} traversals of one player-update (iteration 1, player 0) per step, oracle threads={cores}"
+        desc = "per step: " + cpu_sample_text(sample, info, vpt)
         print(json.dumps({
             "impl": "reference", "metric": metric, "value": v, "unit": "traversals/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / max(1, args.steps),
@@ -628,10 +660,11 @@ def main():
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sample = {"6max-100bb": 2048, "6max-100bb-refrule": 65536, "hu-20bb": 16384}.get(args.workload, 65536)
-        rate, info = cpu_traversal_rate(L, cfg, sample)
+        vpt = visits / max(1, trav)  # this run's timed iterations
+        rate, info = cpu_traversal_rate(L, cfg, sample, vpt)
         out["cpu_baseline"] = {"value": rate, "unit": "traversals/s", "cores": info["cores"], "kind": "port",
-                               "sample": f"{sample} traversals of one player-update (iteration 1, player 0), "
-                                         f"{info['seconds']:.1f} s on {info['cores']} threads"}
+                               "sample": cpu_sample_text(sample, info, vpt),
+                               "raw_traversals_per_s": info["raw_traversals_per_s"]}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
