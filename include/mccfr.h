@@ -157,7 +157,8 @@ typedef struct mccfr_handle mccfr_handle;
 /* ---- configuration ---------------------------------------------------- */
 /* Fills *cfg with a preset; the REF8 preset reproduces the constructor defaults of
    GPUCFRTrainer (cfr_gpu.cuh:50-55): 2 players, stack 1000, blinds 10/20, CFR+ and
-   linear CFR on, the 8 fixed action slots, 64 Chen buckets, 128 rank buckets. */
+   linear CFR on, the 8 fixed action slots, 64 Chen buckets, 128 rank buckets, and
+   one table row per FNV slot (2^26 rows, direct-mapped, 17.2 GB). */
 int mccfr_config_init(mccfr_config* cfg, int preset);
 
 /* ---- lifetime (replaces GPUCFRTrainer::GPUCFRTrainer / ~GPUCFRTrainer,

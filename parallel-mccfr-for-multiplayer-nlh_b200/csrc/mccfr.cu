@@ -749,7 +749,9 @@ int mccfr_config_init(mccfr_config* c, int preset) {
     c->preflop_buckets = 64;
     c->postflop_mode = MCCFR_POSTFLOP_REF_LINEAR;
     c->postflop_buckets[0] = c->postflop_buckets[1] = c->postflop_buckets[2] = 128;
-    c->table_log2 = 24;
+    // one row per FNV slot, direct-mapped like the reference's [8][2^26] arrays
+    // (cfr_gpu.cu:1106-1136): the table never fills
+    c->table_log2 = 26;
     c->seed = 42;  // the reference's hard-wired seed (cfr_gpu.cuh:124)
     return MCCFR_OK;
   }

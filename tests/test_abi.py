@@ -47,6 +47,7 @@ def test_presets():
     ref8 = L.preset(L.PRESET_REF8)
     assert (ref8.num_players, ref8.starting_stack, ref8.small_blind, ref8.big_blind) == (2, 1000, 10, 20)
     assert ref8.num_actions == 8 and ref8.max_depth == 20 and ref8.seed == 42
+    assert ref8.key_mode == L.KEY_FNV26 and ref8.table_log2 == 26  # one row per FNV slot
     assert list(ref8.action_kind) == [0, 1, 2, 4, 5, 5, 5, 6]
     hu = L.preset(L.PRESET_HU_20BB)
     assert hu.num_players == 2 and hu.starting_stack == 20 * hu.big_blind and hu.raise_cap == 2
