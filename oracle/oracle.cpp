@@ -438,13 +438,42 @@ struct Subgame {
   std::vector<uint32_t> cdf;  // [N][1326]
 };
 
+// Rows sharded by key, so that a player-update's fold runs one shard per host
+// thread.  Which shard holds a row changes nothing it computes.
+constexpr int kRowShards = 64;
+static inline int row_shard(uint64_t key) { return (int)((key * 0x9E3779B97F4A7C15ull) >> 58); }
+
+struct RowTable {
+  std::vector<std::unordered_map<uint64_t, Row>> shard =
+      std::vector<std::unordered_map<uint64_t, Row>>(kRowShards);
+  size_t size() const {
+    size_t n = 0;
+    for (const auto& m : shard) n += m.size();
+    return n;
+  }
+  Row& operator[](uint64_t key) { return shard[row_shard(key)][key]; }
+  const Row* find(uint64_t key) const {
+    const auto& m = shard[row_shard(key)];
+    const auto it = m.find(key);
+    return it == m.end() ? nullptr : &it->second;
+  }
+  std::vector<uint64_t> sorted_keys() const {
+    std::vector<uint64_t> ks;
+    ks.reserve(size());
+    for (const auto& m : shard)
+      for (const auto& kv : m) ks.push_back(kv.first);
+    std::sort(ks.begin(), ks.end());
+    return ks;
+  }
+};
+
 struct Oracle {
   Subgame sg;
   Rules R;
   const int32_t* T = nullptr;
   uint8_t pre_lut[52 * 52];
   uint8_t cdf_lut[3][7463];
-  std::unordered_map<uint64_t, Row> rows;
+  RowTable rows;
   bool float_mode = false;
   int64_t iterations_done = 0;
   Counters total;
@@ -475,16 +504,13 @@ struct Ctx {
   uint32_t t;       // traversal index
   uint32_t launch;  // (iteration-1)*N + player
   int rb;
-  std::unordered_map<uint64_t, Acc>* acc;
+  std::unordered_map<uint64_t, Acc>* acc;  // this thread's accumulators, one map per row shard
   Counters* cnt;
   mccfr_trace* trace;
   float w;
 };
 
-static inline const Row* find_row(const Oracle& O, uint64_t key) {
-  const auto it = O.rows.find(key);
-  return it == O.rows.end() ? nullptr : &it->second;
-}
+static inline const Row* find_row(const Oracle& O, uint64_t key) { return O.rows.find(key); }
 
 static uint64_t info_key(const Oracle& O, const Game& g, int player) {
   int hb = g.hole_b[player];
@@ -614,7 +640,7 @@ static float showdown(const Game& g, int up) {  // cfr_gpu.cu:694-753
 
 static void record_node(Ctx& C, uint64_t key, uint8_t vm, const float* rdelta, const float* strat,
                         bool has_r, bool has_s) {
-  Acc& A = (*C.acc)[key];
+  Acc& A = C.acc[row_shard(key)][key];
   A.visits++;
   for (int a = 0; a < 8; ++a) {
     if (!(vm & (1u << a))) continue;
@@ -720,7 +746,7 @@ static float traverse(Ctx& C, Game& g, int depth) {  // cfr_gpu.cu:644-860
     for (int a = 0; a < 8; ++a)
       if (vm & (1u << a)) vh = vh + strat[a] * v[a];
     // Regret delta of action a: fix(v[a]) - fix(v_h), exact in fixed point.
-    Acc& A = (*C.acc)[key];
+    Acc& A = C.acc[row_shard(key)][key];
     A.visits++;
     const int64_t fvh = fix_r(vh, C.rb);
     for (int a = 0; a < 8; ++a) {
@@ -977,17 +1003,18 @@ static int step(Oracle& O, long long iteration, int player, int batch, mccfr_tra
   const float w = R.c.use_linear_cfr ? (float)iteration : 1.0f;
   if (nthreads < 1) nthreads = 1;
   if (O.float_mode) nthreads = 1;
-  std::vector<std::unordered_map<uint64_t, Acc>> accs(nthreads);
+  std::vector<std::vector<std::unordered_map<uint64_t, Acc>>> accs(
+      nthreads, std::vector<std::unordered_map<uint64_t, Acc>>(kRowShards));
   std::vector<Counters> cnts(nthreads);
   // Float mode keeps per-row FP32 sums in traversal order, so it runs on one thread.
   std::atomic<int> next{0};
   auto worker = [&](int tid) {
     for (;;) {
-      const int b = next.fetch_add(256);
+      const int b = next.fetch_add(32);
       if (b >= batch) break;
-      const int e = std::min(batch, b + 256);
+      const int e = std::min(batch, b + 32);
       for (int t = b; t < e; ++t) {
-        Ctx C{&O, player, (uint32_t)t, launch, rb, &accs[tid], &cnts[tid],
+        Ctx C{&O, player, (uint32_t)t, launch, rb, accs[tid].data(), &cnts[tid],
               trace ? &trace[t] : nullptr, w};
         run_traversal(C);
       }
@@ -1000,19 +1027,6 @@ static int step(Oracle& O, long long iteration, int player, int batch, mccfr_tra
     for (int i = 0; i < nthreads; ++i) th.emplace_back(worker, i);
     for (auto& x : th) x.join();
   }
-  // Merge (integer sums: order-independent).
-  std::unordered_map<uint64_t, Acc> all;
-  for (auto& m : accs)
-    for (auto& kv : m) {
-      Acc& A = all[kv.first];
-      for (int a = 0; a < 8; ++a) {
-        A.dr[a] += kv.second.dr[a];
-        A.ds[a] += kv.second.ds[a];
-        A.fr[a] += kv.second.fr[a];
-        A.fs[a] += kv.second.fs[a];
-      }
-      A.visits += kv.second.visits;
-    }
   for (auto& c : cnts) {
     O.total.V += c.V;
     O.total.U += c.U;
@@ -1020,28 +1034,60 @@ static int step(Oracle& O, long long iteration, int player, int batch, mccfr_tra
     O.total.E += c.E;
     O.total.X += c.X;
   }
-  // Apply: the sparse equivalent of the CFR+ clamp sweep (cfr_gpu.cu:1018-1022),
-  // over rows touched by this player-update only.
+  // Fold, shard by shard on the same threads: merge the threads' accumulators
+  // (integer sums: order-independent), then apply them, the sparse equivalent of
+  // the CFR+ clamp sweep (cfr_gpu.cu:1018-1022) over the rows this update touched.
   const double sr = std::ldexp(1.0, -rb);
   const double ss = std::ldexp(1.0, -32);
-  for (auto& kv : all) {
-    Row& row = O.rows[kv.first];
-    const Acc& A = kv.second;
-    for (int a = 0; a < 8; ++a) {
-      float r;
-      float s;
-      if (O.float_mode) {
-        r = row.r[a] + A.fr[a];
-        s = row.s[a] + A.fs[a];
-      } else {
-        r = row.r[a] + (float)((double)A.dr[a] * sr);
-        s = row.s[a] + (float)((double)A.ds[a] * ss * (double)w);
+  auto apply = [&](std::unordered_map<uint64_t, Row>& rows, const std::unordered_map<uint64_t, Acc>& all) {
+    for (const auto& kv : all) {
+      Row& row = rows[kv.first];
+      const Acc& A = kv.second;
+      for (int a = 0; a < 8; ++a) {
+        float r;
+        float s;
+        if (O.float_mode) {
+          r = row.r[a] + A.fr[a];
+          s = row.s[a] + A.fs[a];
+        } else {
+          r = row.r[a] + (float)((double)A.dr[a] * sr);
+          s = row.s[a] + (float)((double)A.ds[a] * ss * (double)w);
+        }
+        if (R.c.use_cfr_plus) r = (r < 0.0f) ? 0.0f : r;
+        row.r[a] = r;
+        row.s[a] = s;
       }
-      if (R.c.use_cfr_plus) r = (r < 0.0f) ? 0.0f : r;
-      row.r[a] = r;
-      row.s[a] = s;
+      row.visits += A.visits;
     }
-    row.visits += A.visits;
+  };
+  std::atomic<int> next_shard{0};
+  auto fold = [&]() {
+    for (int sh; (sh = next_shard.fetch_add(1)) < kRowShards;) {
+      if (nthreads == 1) {
+        apply(O.rows.shard[sh], accs[0][sh]);
+        continue;
+      }
+      std::unordered_map<uint64_t, Acc> all;
+      for (auto& per_thread : accs)
+        for (const auto& kv : per_thread[sh]) {
+          Acc& A = all[kv.first];
+          for (int a = 0; a < 8; ++a) {
+            A.dr[a] += kv.second.dr[a];
+            A.ds[a] += kv.second.ds[a];
+            A.fr[a] += kv.second.fr[a];
+            A.fs[a] += kv.second.fs[a];
+          }
+          A.visits += kv.second.visits;
+        }
+      apply(O.rows.shard[sh], all);
+    }
+  };
+  if (nthreads == 1) {
+    fold();
+  } else {
+    std::vector<std::thread> th;
+    for (int i = 0; i < nthreads; ++i) th.emplace_back(fold);
+    for (auto& x : th) x.join();
   }
   return 0;
 }
@@ -1144,10 +1190,7 @@ void orc_counters(void* h, int64_t* out) {
 int orc_export_rows(void* h, uint64_t* keys, float* R, float* S, uint64_t* visits, size_t cap,
                     size_t* count) {
   Oracle& O = *(Oracle*)h;
-  std::vector<uint64_t> ks;
-  ks.reserve(O.rows.size());
-  for (auto& kv : O.rows) ks.push_back(kv.first);
-  std::sort(ks.begin(), ks.end());
+  const std::vector<uint64_t> ks = O.rows.sorted_keys();
   *count = ks.size();
   if (cap < ks.size()) return MCCFR_ERR_CAPACITY;
   for (size_t i = 0; i < ks.size(); ++i) {
@@ -1164,9 +1207,7 @@ int orc_export_rows(void* h, uint64_t* keys, float* R, float* S, uint64_t* visit
 int orc_get_strategy(void* h, uint32_t* keys, uint64_t* keys64, float* probs, size_t cap,
                      size_t* count) {
   Oracle& O = *(Oracle*)h;
-  std::vector<uint64_t> ks;
-  for (auto& kv : O.rows) ks.push_back(kv.first);
-  std::sort(ks.begin(), ks.end());
+  const std::vector<uint64_t> ks = O.rows.sorted_keys();
   std::vector<std::pair<uint64_t, std::array<float, 8>>> out;
   for (uint64_t k : ks) {
     const Row& r = O.rows[k];
