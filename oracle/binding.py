@@ -14,6 +14,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_LIB = HERE / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libref.so"
+REF_EVAL_LIB = HERE / "_ref" / "libref_eval.so"
 
 
 def _p(a: np.ndarray) -> c_void_p:
@@ -197,3 +198,51 @@ def ref() -> ctypes.CDLL:
         r.ref_abstraction_init()
         _ref = r
     return _ref
+
+
+_ref_eval = None
+
+# OpponentType of the reference's eval.h, in order.
+OPPONENTS = ("calling_station", "nit", "maniac", "balanced", "random")
+
+
+def ref_eval_available() -> bool:
+    return REF_EVAL_LIB.exists()
+
+
+def ref_eval() -> ctypes.CDLL:
+    """The reference's strategy loader and scripted-opponent evaluator
+    (strategy.cpp, eval.cpp), compiled unchanged by oracle/Makefile."""
+    global _ref_eval
+    if _ref_eval is None:
+        r = ctypes.CDLL(str(REF_EVAL_LIB))
+        r.refeval_init.argtypes = [c_char_p]
+        r.refeval_load.argtypes = [c_char_p]
+        r.refeval_load.restype = c_longlong
+        r.refeval_entry.argtypes = [c_uint32, c_void_p]
+        r.refeval_play.argtypes = [c_int, c_int, c_longlong, c_int, c_int, c_int, ctypes.c_uint,
+                                   POINTER(ctypes.c_double), POINTER(ctypes.c_double), POINTER(c_longlong)]
+        _ref_eval = r
+    return _ref_eval
+
+
+def ref_play(opponent: str, n_hands: int, n_players: int = 2, stack: int = 1000, sb: int = 10, bb: int = 20,
+             seed: int = 42) -> dict:
+    """evaluate_strategy_np on the strategy loaded by ref_eval().refeval_load."""
+    b100, net, hands = ctypes.c_double(), ctypes.c_double(), c_longlong()
+    ref_eval().refeval_play(n_players, OPPONENTS.index(opponent), n_hands, stack, sb, bb, seed,
+                            ctypes.byref(b100), ctypes.byref(net), ctypes.byref(hands))
+    return {"bb_per_100": b100.value, "net_bb": net.value, "hands": hands.value}
+
+
+def write_strategy_v2(path, keys32: np.ndarray, probs: np.ndarray) -> None:
+    """The v2 strategy dump mccfr_save_strategy writes (include/mccfr.h):
+    [u64 magic][u32 2^26][u32 8][u32 n] then n x {u32 key, f32[8]}, keys ascending."""
+    order = np.argsort(keys32, kind="stable")
+    rec = np.zeros(len(keys32), dtype=np.dtype([("k", np.uint32), ("p", np.float32, 8)]))
+    rec["k"] = keys32[order]
+    rec["p"] = probs[order]
+    with open(path, "wb") as f:
+        f.write(np.array([0x53545241540100], np.uint64).tobytes())
+        f.write(np.array([1 << 26, 8, len(rec)], np.uint32).tobytes())
+        f.write(rec.tobytes())
