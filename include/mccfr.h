@@ -220,6 +220,16 @@ int mccfr_import_tables(mccfr_handle* h, const float* regrets,
    [u32 8] regrets[8][2^26] strategy_sum[8][2^26] (FNV26 mode only). */
 int mccfr_save_checkpoint(mccfr_handle* h, const char* path);
 int mccfr_load_checkpoint(mccfr_handle* h, const char* path);
+/* Checkpoint v2, any key mode: [u64 "MCCFRCK2"][u32 2][u32 sizeof(mccfr_config)]
+   [mccfr_config][i64 iterations done][u64 rows] then per row {u64 key,
+   f32 regrets[8], f32 strategy_sum[8], u64 visits}, keys ascending.  Unlike the
+   reference's checkpoint it keeps the iteration count and the seed, so training
+   resumed from it equals uninterrupted training bit for bit.  Loading replaces
+   the table's contents and the iteration count; it refuses a file written for a
+   different game or abstraction (every config field but device and table_log2)
+   and keys that cannot belong to this table. */
+int mccfr_save_checkpoint_v2(mccfr_handle* h, const char* path);
+int mccfr_load_checkpoint_v2(mccfr_handle* h, const char* path);
 /* Strategy dump v2: [u64 0x53545241540100][u32 2^26][u32 8][u32 n]{u32 key, f32[8]}. */
 int mccfr_save_strategy(mccfr_handle* h, const char* path);
 

@@ -101,7 +101,8 @@ int main(int argc, char** argv) {
     if (mode == "train") {
       GPUCFRTrainer* t = make();
       if (!t) return 1;
-      if (!load.empty() && !t->load_checkpoint(load)) fprintf(stderr, "WARNING: could not load checkpoint %s\n", load.c_str());
+      if (!load.empty() && !t->load_checkpoint(load) && mccfr_load_checkpoint_v2(t->handle(), load.c_str()) != MCCFR_OK)
+        fprintf(stderr, "WARNING: could not load checkpoint %s\n", load.c_str());
       printf("Training: players=%d iters=%lld batch=%d\n", c.num_players, iters, batch);
       const auto t0 = std::chrono::steady_clock::now();
       t->train(iters, batch, true, save.empty() ? "" : save + ".ckpt", 10000);
@@ -109,7 +110,9 @@ int main(int argc, char** argv) {
       printf("Done: %.0fM traversals in %.2fs (%.1fM traversals/s)\n", iters * (double)batch * c.num_players / 1e6, sec,
              iters * (double)batch * c.num_players / sec / 1e6);
       printf("Info sets active: %d\n", t->num_info_sets_active());
-      if (c.key_mode == MCCFR_KEY_FNV26 && t->save_checkpoint(save + ".ckpt")) printf("Checkpoint saved to %s.ckpt\n", save.c_str());
+      if (c.key_mode == MCCFR_KEY_FNV26 ? t->save_checkpoint(save + ".ckpt")
+                                        : mccfr_save_checkpoint_v2(t->handle(), (save + ".ckpt").c_str()) == MCCFR_OK)
+        printf("Checkpoint saved to %s.ckpt\n", save.c_str());
       if (mccfr_save_strategy(t->handle(), save.c_str()) == MCCFR_OK) printf("Strategy saved to %s\n", save.c_str());
       delete t;
     } else if (mode == "benchmark") {

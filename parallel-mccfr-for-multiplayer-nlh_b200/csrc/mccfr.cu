@@ -192,6 +192,23 @@ __global__ void k_import_dense(const TableView tv, const float* __restrict__ dr,
   }
 }
 
+// Rows of a v2 checkpoint into an empty table: each key's row gets its
+// regrets, strategy sums and visit count (keys checked on the host first).
+__global__ void k_import_rows(const TableView tv, const unsigned long long* __restrict__ keys,
+                              const float4* __restrict__ reg, const float4* __restrict__ ssum,
+                              const unsigned long long* __restrict__ visits, unsigned long long n) {
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const long long slot = table_insert(tv, keys[i]);
+    if (slot < 0) continue;  // table_insert raised the table-full flag
+    row_reg(tv, slot)[0] = reg[2 * i];
+    row_reg(tv, slot)[1] = reg[2 * i + 1];
+    row_ssum(tv, slot)[0] = ssum[2 * i];
+    row_ssum(tv, slot)[1] = ssum[2 * i + 1];
+    *row_visits(tv, slot) = visits[i];
+  }
+}
+
 __global__ void k_export_dense(const TableView tv, unsigned long long cap_slots, float* __restrict__ dr,
                                float* __restrict__ ds, unsigned n_slots) {
   for (unsigned long long s = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; s < cap_slots;
@@ -572,6 +589,7 @@ struct HostRow {
   float reg[8], ssum[8];
   unsigned long long visits;
 };
+static_assert(sizeof(HostRow) == 80, "a v2 checkpoint row is 80 bytes");
 
 // Occupied rows (a counting pass over the table).
 int count_rows(mccfr_handle* h, unsigned int* n) {
@@ -1021,7 +1039,8 @@ int mccfr_train(mccfr_handle* h, long long iters, int batch, int verbose, const 
   CK(cudaSetDevice(h->device));
   int rc = ensure_graph(h, batch);
   if (rc) return rc;
-  rc = set_sched(h, h->iterations_done + 1, 0);
+  const long long base = h->iterations_done;  // iterations before this call
+  rc = set_sched(h, base + 1, 0);
   if (rc) return rc;
   const bool timed = (verbose & 2) != 0;
   const auto t0 = std::chrono::steady_clock::now();
@@ -1045,11 +1064,11 @@ int mccfr_train(mccfr_handle* h, long long iters, int batch, int verbose, const 
         // is reset only by the next update's apply)
         unsigned nt[2] = {0, 0};
         CK(cudaMemcpy(nt, h->tv.n_touched, sizeof(nt), cudaMemcpyDeviceToHost));
-        h->touched_last = nt[(uint32_t)((h->iterations_done + i) * np + np - 1) & 1];
+        h->touched_last = nt[(uint32_t)((base + i) * np + np - 1) & 1];
       }
     }
     h->launches += h->cfg.num_players;
-    const long long it = h->iterations_done + i + 1;
+    const long long it = base + i + 1;
     if ((verbose & 1) && (it % 100 == 0 || i + 1 == iters)) {
       CK(cudaStreamSynchronize(h->stream));
       const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -1058,9 +1077,11 @@ int mccfr_train(mccfr_handle* h, long long iters, int batch, int verbose, const 
       fflush(stdout);
     }
     if (ckpt_path && ckpt_path[0] && ckpt_interval > 0 && it % ckpt_interval == 0) {
+      // the reference's layout for its own keys, v2 (with the iteration) otherwise
       CK(cudaStreamSynchronize(h->stream));
       h->iterations_done = it;
-      rc = mccfr_save_checkpoint(h, ckpt_path);
+      rc = h->cfg.key_mode == MCCFR_KEY_FNV26 ? mccfr_save_checkpoint(h, ckpt_path)
+                                              : mccfr_save_checkpoint_v2(h, ckpt_path);
       if (rc) return rc;
       rc = set_sched(h, it + 1, 0);
       if (rc) return rc;
@@ -1068,7 +1089,7 @@ int mccfr_train(mccfr_handle* h, long long iters, int batch, int verbose, const 
   }
   CK(cudaStreamSynchronize(h->stream));
   if (verbose & 1) printf("\n");
-  h->iterations_done += iters;
+  h->iterations_done = base + iters;
   return check_device_error(h);
 }
 
@@ -1269,6 +1290,119 @@ int mccfr_load_checkpoint(mccfr_handle* h, const char* path) {
     CK(cudaStreamSynchronize(h->stream));
   }
   return MCCFR_OK;
+}
+
+// ---- v2 checkpoint (any key mode) -------------------------------------------
+// [u64 "MCCFRCK2"][u32 2][u32 sizeof(mccfr_config)][mccfr_config]
+// [i64 iterations done][u64 rows] rows x {u64 key, f32 regrets[8],
+// f32 strategy_sum[8], u64 visits}, keys ascending.  The reference's checkpoint
+// (cfr_gpu.cu:1464-1538) keeps neither the iteration nor the seed, so linear-CFR
+// weights restart at t = 1 after its resume; with both kept and counter-based
+// draws, training resumed from this file equals uninterrupted training.
+namespace {
+constexpr uint64_t kCkptV2Magic = 0x324B43524643434DULL;  // "MCCFRCK2" little-endian
+
+// The fields that define the game and its abstraction: all but the device and
+// the table capacity.
+bool same_game(mccfr_config a, mccfr_config b) {
+  a.device = b.device = 0;
+  a.table_log2 = b.table_log2 = 0;
+  std::memset(a.reserved, 0, sizeof(a.reserved));
+  std::memset(b.reserved, 0, sizeof(b.reserved));
+  return std::memcmp(&a, &b, sizeof(a)) == 0;
+}
+}  // namespace
+
+int mccfr_save_checkpoint_v2(mccfr_handle* h, const char* path) {
+  if (!h || !path) return MCCFR_ERR_INVALID_ARG;
+  CK(cudaSetDevice(h->device));
+  std::vector<HostRow> rows;
+  const int rc = read_rows(h, rows);
+  if (rc) return rc;
+  FILE* f = fopen(path, "wb");
+  if (!f) return fail(h, MCCFR_ERR_IO, "cannot open %s", path);
+  const uint32_t ver = 2, cfg_bytes = sizeof(mccfr_config);
+  const int64_t iters = h->iterations_done;
+  const uint64_t n = rows.size();
+  bool ok = fwrite(&kCkptV2Magic, 8, 1, f) == 1 && fwrite(&ver, 4, 1, f) == 1 && fwrite(&cfg_bytes, 4, 1, f) == 1 &&
+            fwrite(&h->cfg, sizeof(mccfr_config), 1, f) == 1 && fwrite(&iters, 8, 1, f) == 1 &&
+            fwrite(&n, 8, 1, f) == 1 && (n == 0 || fwrite(rows.data(), sizeof(HostRow), n, f) == n);
+  ok = (fclose(f) == 0) && ok;
+  return ok ? MCCFR_OK : fail(h, MCCFR_ERR_IO, "write %s failed", path);
+}
+
+int mccfr_load_checkpoint_v2(mccfr_handle* h, const char* path) {
+  if (!h || !path) return MCCFR_ERR_INVALID_ARG;
+  FILE* f = fopen(path, "rb");
+  if (!f) return fail(h, MCCFR_ERR_IO, "cannot open %s", path);
+  uint64_t magic = 0, n = 0;
+  uint32_t ver = 0, cfg_bytes = 0;
+  int64_t iters = 0;
+  mccfr_config saved{};
+  bool ok = fread(&magic, 8, 1, f) == 1 && fread(&ver, 4, 1, f) == 1 && fread(&cfg_bytes, 4, 1, f) == 1 &&
+            magic == kCkptV2Magic && ver == 2 && cfg_bytes == sizeof(mccfr_config) &&
+            fread(&saved, sizeof(saved), 1, f) == 1 && fread(&iters, 8, 1, f) == 1 && fread(&n, 8, 1, f) == 1;
+  if (!ok) {
+    fclose(f);
+    return fail(h, MCCFR_ERR_FORMAT, "%s: not a v2 checkpoint", path);
+  }
+  if (!same_game(saved, h->cfg)) {
+    fclose(f);
+    return fail(h, MCCFR_ERR_INVALID_ARG, "%s: written for a different game or abstraction", path);
+  }
+  if (iters < 0 || n > h->cap) {
+    fclose(f);
+    return fail(h, MCCFR_ERR_FORMAT, "%s: %llu rows for a %llu-row table", path, (unsigned long long)n, h->cap);
+  }
+  std::vector<HostRow> rows(n);
+  ok = n == 0 || fread(rows.data(), sizeof(HostRow), n, f) == n;
+  fclose(f);
+  if (!ok) return fail(h, MCCFR_ERR_FORMAT, "%s: truncated checkpoint", path);
+  // Keys must be nonzero, ascending and, in a direct-mapped table, at most the
+  // key space (row key-1 must exist): checked here, before any device write.
+  const int kb = h->cfg.key_mode == MCCFR_KEY_FNV26 ? 26 : h->cfg.key_bits;
+  const unsigned long long kmax = h->tv.direct ? (1ull << kb) : ~0ull;
+  for (uint64_t i = 0; i < n; ++i)
+    if (rows[i].key == 0 || rows[i].key > kmax || (i && rows[i].key <= rows[i - 1].key))
+      return fail(h, MCCFR_ERR_FORMAT, "%s: row %llu has an invalid key", path, (unsigned long long)i);
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaMemsetAsync(h->d_block, 0, h->block_bytes, h->stream));  // rows, touched list, counters
+  int rc = MCCFR_OK;
+  if (n) {
+    std::vector<unsigned long long> keys(n), vis(n);
+    std::vector<float> reg(8 * n), ssum(8 * n);
+    for (uint64_t i = 0; i < n; ++i) {
+      keys[i] = rows[i].key;
+      vis[i] = rows[i].visits;
+      std::memcpy(&reg[8 * i], rows[i].reg, 32);
+      std::memcpy(&ssum[8 * i], rows[i].ssum, 32);
+    }
+    void* block = nullptr;
+    cudaError_t e = cudaMalloc(&block, n * 80);
+    if (e != cudaSuccess) return fail(h, MCCFR_ERR_OOM, "checkpoint upload buffers");
+    char* base = static_cast<char*>(block);
+    float4* d_reg = reinterpret_cast<float4*>(base);
+    float4* d_ssum = reinterpret_cast<float4*>(base + n * 32);
+    unsigned long long* d_keys = reinterpret_cast<unsigned long long*>(base + n * 64);
+    unsigned long long* d_vis = reinterpret_cast<unsigned long long*>(base + n * 72);
+    e = cudaMemcpyAsync(d_reg, reg.data(), n * 32, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_ssum, ssum.data(), n * 32, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_keys, keys.data(), n * 8, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_vis, vis.data(), n * 8, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+      k_import_rows<<<148 * 16, 256, 0, h->stream>>>(h->tv, d_keys, d_reg, d_ssum, d_vis, n);
+      e = cudaStreamSynchronize(h->stream);
+    }
+    cudaFree(block);
+    if (e != cudaSuccess) rc = fail(h, MCCFR_ERR_CUDA, "checkpoint import: %s", cudaGetErrorString(e));
+  }
+  if (!rc) rc = check_device_error(h);
+  if (!rc) {
+    h->iterations_done = iters;
+    h->touched_last = 0;
+  }
+  return rc;
 }
 
 // Strategy dump v2 (strategy.cpp:6-8, 35-52), rows sorted by key.

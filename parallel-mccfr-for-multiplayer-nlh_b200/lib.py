@@ -139,6 +139,8 @@ SIGNATURES = {
     "mccfr_import_tables": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),
     "mccfr_save_checkpoint": (c_int, [c_void_p, c_char_p]),
     "mccfr_load_checkpoint": (c_int, [c_void_p, c_char_p]),
+    "mccfr_save_checkpoint_v2": (c_int, [c_void_p, c_char_p]),
+    "mccfr_load_checkpoint_v2": (c_int, [c_void_p, c_char_p]),
     "mccfr_save_strategy": (c_int, [c_void_p, c_char_p]),
     "mccfr_get_stats": (c_int, [c_void_p, POINTER(Stats)]),
     "mccfr_get_config": (c_int, [c_void_p, POINTER(Config)]),

@@ -129,6 +129,16 @@ class GPUCFRTrainer:
     def load_checkpoint(self, path: str) -> bool:
         return self._lib.mccfr_load_checkpoint(self._h, str(path).encode()) == L.OK
 
+    def save_checkpoint_v2(self, path: str) -> None:
+        """Config, iteration count and every occupied row (mccfr_save_checkpoint_v2)."""
+        L.check(self._lib.mccfr_save_checkpoint_v2(self._h, str(path).encode()), self._h)
+
+    def load_checkpoint_v2(self, path: str) -> None:
+        """Replaces the table and the iteration count; training continues exactly
+        where the saved trainer stopped (mccfr_load_checkpoint_v2)."""
+        L.check(self._lib.mccfr_load_checkpoint_v2(self._h, str(path).encode()), self._h)
+        self.iterations_done = int(self.stats().iterations_done)
+
     def num_info_sets_active(self) -> int:
         n = c_longlong()
         L.check(self._lib.mccfr_num_info_sets_active(self._h, byref(n)), self._h)
