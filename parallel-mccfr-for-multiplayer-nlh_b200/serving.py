@@ -13,6 +13,7 @@ own tables and Philox keys, never on what it was batched with.
 from __future__ import annotations
 
 import math
+import threading
 import time
 from dataclasses import dataclass, field
 
@@ -122,6 +123,7 @@ class Result:
     finished: float
     keys: np.ndarray = field(repr=False)
     probs: np.ndarray = field(repr=False)
+    cancelled: bool = False     # withdrawn by cancel(): no strategy
 
     @property
     def latency_ms(self) -> float:
@@ -138,10 +140,17 @@ class ReSolveServer:
     tables are kept in a pool by capacity and reset for new requests of the
     same capacity (mccfr_subgame_reset), so a steady stream of requests
     allocates and frees no device memory; pooled tables are freed when a new
-    capacity needs the room, and by close()."""
+    capacity needs the room, and by close().
+
+    cancel(rid), from any thread, withdraws a request: one not yet admitted is
+    dropped, one being solved retires after the current round without exporting
+    its strategy, and its table goes back to the pool.  round_fn and create_fn
+    replace the device round (batch_round) and the table creation, so the loop's
+    host logic can run against stand-ins."""
 
     def __init__(self, rank_table_owner: GPUCFRTrainer, hbm_budget: int = 16 << 30, max_active: int = 64,
-                 traversals: int = 256, tuning: dict | None = None, free_memory=None):
+                 traversals: int = 256, tuning: dict | None = None, free_memory=None, round_fn=None,
+                 create_fn=None):
         self.owner = rank_table_owner
         self.hbm_budget = int(hbm_budget)
         self.max_active = min(64, int(max_active))
@@ -153,6 +162,24 @@ class ReSolveServer:
         self.timing = {"admit_s": 0.0, "round_s": 0.0, "retire_s": 0.0}
         self.pool: dict[int, list[GPUCFRTrainer]] = {}
         self.reused = 0
+        self.cancelled = 0
+        self._round = round_fn or batch_round
+        self._create = create_fn or self._create_subgame
+        self._lock = threading.Lock()
+        self._withdrawn: set[int] = set()
+
+    def cancel(self, rid: int) -> None:
+        with self._lock:
+            self._withdrawn.add(int(rid))
+
+    def _is_cancelled(self, rid: int) -> bool:
+        with self._lock:
+            return rid in self._withdrawn
+
+    def _create_subgame(self, cfg: L.Config, req: Request) -> GPUCFRTrainer:
+        t = GPUCFRTrainer.subgame(cfg, req.street, req.pot, req.board, req.ranges)
+        t.share_hand_table(self.owner)
+        return t
 
     @staticmethod
     def _device_free() -> int:
@@ -186,8 +213,7 @@ class ReSolveServer:
             t.reset_subgame(cfg, req.street, req.pot, req.board, req.ranges)
             self.reused += 1
         else:
-            t = GPUCFRTrainer.subgame(cfg, req.street, req.pot, req.board, req.ranges)
-            t.share_hand_table(self.owner)
+            t = self._create(cfg, req)
         per_player = max(1, math.ceil(req.budget / self.traversals))
         return Solve(req, t, per_player * req.players, admitted=now)
 
@@ -207,10 +233,19 @@ class ReSolveServer:
         held = 0
         results: list[Result] = []
         t0 = time.perf_counter()
+        none = np.zeros(0, np.uint32), np.zeros((0, 8), np.float32)
+
+        def withdraw(req: Request, admitted: float) -> None:
+            self.cancelled += 1
+            results.append(Result(req.rid, req.arrival, admitted, time.perf_counter() - t0, *none, cancelled=True))
+
         while pending or queue or active:
             now = time.perf_counter() - t0
             while pending and (not realtime or pending[0].arrival <= now):
                 queue.append(pending.pop(0))
+            for req in [r for r in queue if self._is_cancelled(r.rid)]:
+                queue.remove(req)
+                withdraw(req, now)
             ta = time.perf_counter()
             while queue and self.admit_ok(queue[0], held, len(active)):
                 req = queue.pop(0)
@@ -222,14 +257,18 @@ class ReSolveServer:
                     time.sleep(max(0.0, min(0.001, pending[0].arrival - now)))
                 continue
             tr = time.perf_counter()
-            batch_round([s.trainer for s in active], [self.traversals] * len(active), self.tuning)
+            self._round([s.trainer for s in active], [self.traversals] * len(active), self.tuning)
             self.rounds += 1
             tz = time.perf_counter()
             self.timing["round_s"] += tz - tr
             still = []
             for s in active:
                 s.updates_done += 1
-                if s.updates_done >= s.updates_needed:
+                if self._is_cancelled(s.req.rid):
+                    withdraw(s.req, s.admitted)
+                    self.pool.setdefault(s.req.table_log2, []).append(s.trainer)
+                    held -= table_bytes(s.req)
+                elif s.updates_done >= s.updates_needed:
                     keys, probs = s.trainer.strategy_arrays()
                     results.append(Result(s.req.rid, s.req.arrival, s.admitted, time.perf_counter() - t0, keys, probs))
                     self.pool.setdefault(s.req.table_log2, []).append(s.trainer)  # kept for the next request

@@ -82,3 +82,95 @@ def test_pool_reuse_and_eviction():
     assert not srv.admit_ok(req, 2 * need, 0)     # no room even with the pool empty
     srv.close()
     assert srv.pool == {}
+
+
+class _FakeSolver:
+    """Stands in for a subgame trainer: counts its rounds and resets."""
+
+    def __init__(self):
+        self.closed = False
+        self.rounds = 0
+        self.resets = 0
+
+    def reset_subgame(self, *args):
+        self.resets += 1
+        self.rounds = 0
+
+    def strategy_arrays(self):
+        return np.array([7], np.uint32), np.full((1, 8), 0.125, np.float32)
+
+    def close(self):
+        self.closed = True
+
+
+def _same_size_requests(n: int) -> list:
+    rng = np.random.default_rng(5)
+    reqs = [sv.make_request(rng, rid) for rid in range(n)]
+    for r in reqs:
+        r.table_log2, r.budget, r.players = 16, 4 * 256, 2  # 4 rounds per player, 8 rounds each
+    return reqs
+
+
+def test_cancel_before_admission_and_mid_solve():
+    """A request withdrawn while queued never gets a table; one withdrawn
+    mid-solve retires after that round with no strategy, and its table is reused
+    by the next request.  The others finish with their full budgets."""
+    reqs = _same_size_requests(4)
+    made = []
+    rounds = [0]
+
+    def create(cfg, req):
+        made.append(_FakeSolver())
+        return made[-1]
+
+    def round_fn(trainers, traversals, tuning):
+        rounds[0] += 1
+        for t in trainers:
+            t.rounds += 1
+        if rounds[0] == 3:
+            srv.cancel(reqs[0].rid)  # a client withdraws mid-solve
+
+    need = sv.table_bytes(reqs[0])
+    srv = sv.ReSolveServer(None, hbm_budget=4 * need, max_active=2, free_memory=lambda: 100 << 30,
+                           traversals=256, round_fn=round_fn, create_fn=create)
+    srv.cancel(reqs[3].rid)  # withdrawn before it is admitted
+    res = {r.rid: r for r in srv.run(reqs, realtime=False)}
+    assert set(res) == {r.rid for r in reqs}
+    assert res[reqs[0].rid].cancelled and res[reqs[0].rid].keys.size == 0
+    assert res[reqs[3].rid].cancelled
+    for r in (reqs[1], reqs[2]):
+        assert not res[r.rid].cancelled and res[r.rid].keys.tolist() == [7]
+    assert srv.cancelled == 2
+    # two tables were made; request 2 ran on request 0's returned table
+    assert len(made) == 2 and srv.reused == 1
+    assert made[0].resets == 1
+    srv.close()
+    assert all(t.closed for t in made)
+
+
+def test_cancel_from_another_thread_is_safe():
+    import threading
+
+    reqs = _same_size_requests(3)
+    started, withdrawn = threading.Event(), threading.Event()
+
+    def round_fn(trainers, traversals, tuning):
+        if not started.is_set():
+            started.set()
+            assert withdrawn.wait(5)  # the first round ends after the other thread's cancel
+        for t in trainers:
+            t.rounds += 1
+
+    def client():
+        assert started.wait(5)
+        srv.cancel(reqs[2].rid)
+        withdrawn.set()
+
+    srv = sv.ReSolveServer(None, hbm_budget=1 << 40, max_active=1, free_memory=lambda: 100 << 30,
+                           traversals=256, round_fn=round_fn, create_fn=lambda cfg, req: _FakeSolver())
+    th = threading.Thread(target=client)
+    th.start()
+    res = {r.rid: r for r in srv.run(reqs, realtime=False)}
+    th.join()
+    assert res[reqs[2].rid].cancelled  # still queued behind the single slot when withdrawn
+    assert not res[reqs[0].rid].cancelled and not res[reqs[1].rid].cancelled
