@@ -160,6 +160,10 @@ typedef struct mccfr_handle mccfr_handle;
    linear CFR on, the 8 fixed action slots, 64 Chen buckets, 128 rank buckets, and
    one table row per FNV slot (2^26 rows, direct-mapped, 17.2 GB). */
 int mccfr_config_init(mccfr_config* cfg, int preset);
+/* Checks a config without a device: MCCFR_OK, or MCCFR_ERR_INVALID_ARG with the
+   first rule it breaks written to why (NUL-terminated, at most why_len bytes;
+   why may be NULL).  mccfr_create applies the same checks. */
+int mccfr_config_validate(const mccfr_config* cfg, char* why, size_t why_len);
 
 /* ---- lifetime (replaces GPUCFRTrainer::GPUCFRTrainer / ~GPUCFRTrainer,
         cfr_gpu.cu:1064-1084) ------------------------------------------- */

@@ -819,6 +819,18 @@ int mccfr_config_init(mccfr_config* c, int preset) {
   return MCCFR_ERR_INVALID_ARG;
 }
 
+int mccfr_config_validate(const mccfr_config* cfg, char* why, size_t why_len) {
+  if (!cfg) return MCCFR_ERR_INVALID_ARG;
+  std::string msg;
+  const bool bad = validate(*cfg, msg) != 0;
+  if (why && why_len) {
+    const size_t n = std::min(why_len - 1, bad ? msg.size() : (size_t)0);
+    std::memcpy(why, msg.data(), n);
+    why[n] = 0;
+  }
+  return bad ? MCCFR_ERR_INVALID_ARG : MCCFR_OK;
+}
+
 int mccfr_create(const mccfr_config* cfg, mccfr_handle** out) {
   if (!cfg || !out) return MCCFR_ERR_INVALID_ARG;
   *out = nullptr;

@@ -123,6 +123,7 @@ assert TRACE_DTYPE.itemsize == ctypes.sizeof(Trace), (TRACE_DTYPE.itemsize, ctyp
 # Every function declared in include/mccfr.h: name -> (restype, argtypes)
 SIGNATURES = {
     "mccfr_config_init": (c_int, [POINTER(Config), c_int]),
+    "mccfr_config_validate": (c_int, [POINTER(Config), ctypes.c_char_p, c_size_t]),
     "mccfr_create": (c_int, [POINTER(Config), POINTER(c_void_p)]),
     "mccfr_destroy": (None, [c_void_p]),
     "mccfr_load_hand_table": (c_int, [c_void_p, c_char_p]),
@@ -209,6 +210,13 @@ def preset(p: int) -> Config:
     cfg = Config()
     check(load().mccfr_config_init(ctypes.byref(cfg), p))
     return cfg
+
+
+def validate(cfg: Config) -> str | None:
+    """None for a valid config, else the first rule it breaks (no device needed)."""
+    why = ctypes.create_string_buffer(256)
+    rc = load().mccfr_config_validate(ctypes.byref(cfg), why, len(why))
+    return None if rc == OK else why.value.decode()
 
 
 def ptr(a: np.ndarray) -> c_void_p:

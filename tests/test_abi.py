@@ -88,3 +88,23 @@ def test_create_without_gpu_fails_cleanly():
         assert e.status == L.ERR_NO_DEVICE
     else:
         raise AssertionError("expected MccfrError")
+
+
+def test_config_validation_without_device():
+    for p in (L.PRESET_REF8, L.PRESET_HU_20BB, L.PRESET_6MAX_100BB):
+        assert L.validate(L.preset(p)) is None
+    cases = [
+        (lambda c: setattr(c, "num_players", 7), "players"),
+        (lambda c: setattr(c, "table_log2", 9), "table_log2"),
+        (lambda c: setattr(c, "key_bits", 60), "key_bits"),
+        (lambda c: setattr(c, "max_depth", 0), "max_depth"),
+    ]
+    for mutate, word in cases:
+        c = L.preset(L.PRESET_HU_20BB)
+        mutate(c)
+        why = L.validate(c)
+        assert why is not None and word in why, (word, why)
+    c = L.preset(L.PRESET_HU_20BB)
+    c.action_kind[0] = L.ACT_CALL  # no fold slot left
+    assert "fold" in L.validate(c)
+
