@@ -15,6 +15,8 @@ abstraction preset that the reference hard-wires.
 from __future__ import annotations
 
 import ctypes
+import json
+import time
 from ctypes import byref, c_longlong, c_size_t, c_void_p
 
 import numpy as np
@@ -113,11 +115,21 @@ class GPUCFRTrainer:
         L.check(self._lib.mccfr_set_hand_table(self._h, L.ptr(t), t.size), self._h)
 
     def train(self, total_iterations: int, batch_size: int = 65536, verbose: bool = True,
-              ckpt_path: str = "", ckpt_interval: int = 10000, timed: bool = False) -> None:
+              ckpt_path: str = "", ckpt_interval: int = 10000, timed: bool = False,
+              metrics: str | None = None) -> None:
+        """As the reference's train.  metrics: a JSON-lines file that gets one
+        line for this call (metrics_line), with the kernels timed on the device."""
+        timed = timed or metrics is not None
+        s0 = self.stats() if metrics else None
+        t0 = time.perf_counter()
         flags = (1 if verbose else 0) | (2 if timed else 0)
         L.check(self._lib.mccfr_train(self._h, int(total_iterations), int(batch_size), flags,
                                       ckpt_path.encode(), int(ckpt_interval)), self._h)
         self.iterations_done += int(total_iterations)
+        if metrics:
+            line = metrics_line(s0, self.stats(), time.perf_counter() - t0, int(total_iterations), int(batch_size))
+            with open(metrics, "a") as f:
+                f.write(json.dumps(line) + "\n")
 
     def get_strategy(self) -> dict[int, np.ndarray]:
         keys, probs = self.strategy_arrays()
@@ -298,3 +310,34 @@ def batch_round(trainers: list, traversals: list[int], tuning: dict | None = Non
         tp = byref(L.BatchTuning(tuning.get("block", 128), tuning.get("grab", 1), tuning.get("smem_frames", 0),
                                  tuning.get("probe_width", 1), tuning.get("warp_sync", 1)))
     L.check(lib.mccfr_batch_round(arr, len(trainers), cnt, tp))
+
+
+def metrics_line(s0, s1, wall_s: float, iterations: int, batch: int) -> dict:
+    """One JSON-lines record of a train() call from the stats before and after
+    it: work counted on the device, rates over the call's wall time, and the
+    kernels' CUDA-event times.  algorithmic_gbs is 40 B per node visit plus 96 B
+    per updating-player update (key + regret row read; regret write, strategy
+    row read and write) over the traversal kernels' time."""
+    trav = s1.traversals - s0.traversals
+    visits = s1.node_visits - s0.node_visits
+    updates = s1.traverser_updates - s0.traverser_updates
+    launches = max(1, s1.launches - s0.launches)
+    tms = s1.traverse_ms - s0.traverse_ms
+    ams = s1.apply_ms - s0.apply_ms
+    return {
+        "time": time.time(),
+        "iteration": int(s1.iterations_done),
+        "iterations": iterations,
+        "traversals_per_update": batch,
+        "wall_s": wall_s,
+        "traversals": int(trav),
+        "traversals_per_s": trav / wall_s if wall_s > 0 else None,
+        "node_visits_per_s": visits / wall_s if wall_s > 0 else None,
+        "hand_evals_per_s": (s1.hand_evals - s0.hand_evals) / wall_s if wall_s > 0 else None,
+        "traverse_ms_per_update": tms / launches,
+        "apply_ms_per_update": ams / launches,
+        "algorithmic_gbs": (40.0 * visits + 96.0 * updates) / (tms / 1e3) / 1e9 if tms > 0 else None,
+        "touched_rows_last_update": int(s1.touched_last),
+        "device_error": int(s1.device_error),
+    }
+

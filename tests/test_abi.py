@@ -8,6 +8,7 @@ import subprocess
 from pathlib import Path
 
 import numpy as np
+import pytest
 
 from conftest import ROOT, gpu_available, mccfr
 
@@ -108,3 +109,21 @@ def test_config_validation_without_device():
     c.action_kind[0] = L.ACT_CALL  # no fold slot left
     assert "fold" in L.validate(c)
 
+
+
+def test_metrics_line_from_stats_snapshots():
+    import importlib
+    from types import SimpleNamespace
+
+    tm = importlib.import_module("mccfr_b200.trainer")
+    s0 = SimpleNamespace(traversals=100, node_visits=1000, traverser_updates=200, hand_evals=300, launches=6,
+                         traverse_ms=10.0, apply_ms=2.0, iterations_done=1, touched_last=5, device_error=0)
+    s1 = SimpleNamespace(traversals=2100, node_visits=101000, traverser_updates=20200, hand_evals=4300,
+                         launches=10, traverse_ms=30.0, apply_ms=6.0, iterations_done=3, touched_last=77,
+                         device_error=0)
+    m = tm.metrics_line(s0, s1, 2.0, 2, 1000)
+    assert m["iteration"] == 3 and m["traversals"] == 2000 and m["traversals_per_s"] == 1000.0
+    assert m["node_visits_per_s"] == 50000.0 and m["hand_evals_per_s"] == 2000.0
+    assert m["traverse_ms_per_update"] == 5.0 and m["apply_ms_per_update"] == 1.0
+    assert m["algorithmic_gbs"] == pytest.approx((40 * 100000 + 96 * 20000) / 0.020 / 1e9)
+    assert m["touched_rows_last_update"] == 77

@@ -104,3 +104,21 @@ def test_table_full_is_reported(hand_table):
         tr.step(1, 0, 2048)
     assert e.value.status == ERR_TABLE_FULL
     tr.close()
+
+
+def test_train_writes_metrics_lines(hand_table, tmp_path):
+    import json
+
+    cfg = L.preset(L.PRESET_HU_20BB)
+    cfg.table_log2, cfg.key_bits = 20, 19
+    tr = mccfr.GPUCFRTrainer(config=cfg)
+    tr.set_hand_table(hand_table)
+    log = tmp_path / "metrics.jsonl"
+    tr.train(2, 1024, verbose=False, metrics=str(log))
+    tr.train(1, 1024, verbose=False, metrics=str(log))
+    lines = [json.loads(x) for x in log.read_text().splitlines()]
+    assert [m["iteration"] for m in lines] == [2, 3]
+    assert [m["traversals"] for m in lines] == [2 * 2 * 1024, 2 * 1024]
+    for m in lines:
+        assert m["traverse_ms_per_update"] > 0 and m["traversals_per_s"] > 0 and m["device_error"] == 0
+    tr.close()
