@@ -513,7 +513,7 @@ def main():
         if rank != 0:
             return
         # bounded per-step samples of the same workload on all host cores
-        sample = {"6max-100bb": 8192, "6max-100bb-refrule": 65536, "hu-20bb": 16384}.get(args.workload, 65536)
+        sample = {"6max-100bb": 16384, "6max-100bb-refrule": 65536, "hu-20bb": 16384}.get(args.workload, 65536)
         vpt = work_per_traversal(args.workload)
         for _ in range(args.warmup):
             cpu_traversal_rate(L, cfg, max(64, sample // 8), vpt)
@@ -659,7 +659,7 @@ def main():
         out["extras"] = extras
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sample = {"6max-100bb": 8192, "6max-100bb-refrule": 65536, "hu-20bb": 16384}.get(args.workload, 65536)
+        sample = {"6max-100bb": 16384, "6max-100bb-refrule": 65536, "hu-20bb": 16384}.get(args.workload, 65536)
         vpt = visits / max(1, trav)  # this run's timed iterations
         rate, info = cpu_traversal_rate(L, cfg, sample, vpt)
         out["cpu_baseline"] = {"value": rate, "unit": "traversals/s", "cores": info["cores"], "kind": "port",

@@ -25,7 +25,6 @@
 #include <cstring>
 #include <mutex>
 #include <thread>
-#include <unordered_map>
 #include <vector>
 
 #include "../include/mccfr.h"
@@ -438,30 +437,77 @@ struct Subgame {
   std::vector<uint32_t> cdf;  // [N][1326]
 };
 
+// Map from nonzero 64-bit keys: an open-addressing slot table (linear probing,
+// load at most 1/2) over dense key and value arrays; the oracle's rows and its
+// per-thread accumulators.  Iteration order is
+// unspecified and never changes a result: sums are integers, rows fold
+// independently and exports are sorted by key.
+template <class V>
+class FlatMap {
+ public:
+  size_t size() const { return vals_.size(); }
+  // A reference stays valid until the next insertion.
+  V& operator[](uint64_t key) {
+    if (2 * (vals_.size() + 1) > slots_.size()) grow();
+    Slot& sl = slots_[slot(key)];
+    if (!sl.key) {
+      sl = Slot{key, (uint32_t)vals_.size()};
+      keys_.push_back(key);
+      vals_.emplace_back();
+    }
+    return vals_[sl.idx];
+  }
+  const V* find(uint64_t key) const {
+    if (slots_.empty()) return nullptr;
+    const Slot& sl = slots_[slot(key)];
+    return sl.key ? &vals_[sl.idx] : nullptr;
+  }
+  template <class F>
+  void each(F f) const {
+    for (size_t j = 0; j < vals_.size(); ++j) f(keys_[j], vals_[j]);
+  }
+
+ private:
+  struct Slot {
+    uint64_t key;  // 0 = empty
+    uint32_t idx;  // into keys_ / vals_
+  };
+  std::vector<Slot> slots_;
+  std::vector<uint64_t> keys_;  // insertion order
+  std::vector<V> vals_;
+
+  // The key's slot, or the empty slot where it belongs.
+  size_t slot(uint64_t key) const {
+    const size_t mask = slots_.size() - 1;
+    size_t i = (size_t)mix64(key) & mask;
+    while (slots_[i].key && slots_[i].key != key) i = (i + 1) & mask;
+    return i;
+  }
+  // Doubles the slot table and re-inserts the keys; values do not move.
+  void grow() {
+    slots_.assign(slots_.empty() ? 64 : 2 * slots_.size(), Slot{0, 0});
+    for (size_t j = 0; j < keys_.size(); ++j) slots_[slot(keys_[j])] = Slot{keys_[j], (uint32_t)j};
+  }
+};
+
 // Rows sharded by key, so that a player-update's fold runs one shard per host
 // thread.  Which shard holds a row changes nothing it computes.
 constexpr int kRowShards = 64;
 static inline int row_shard(uint64_t key) { return (int)((key * 0x9E3779B97F4A7C15ull) >> 58); }
 
 struct RowTable {
-  std::vector<std::unordered_map<uint64_t, Row>> shard =
-      std::vector<std::unordered_map<uint64_t, Row>>(kRowShards);
+  std::vector<FlatMap<Row>> shard = std::vector<FlatMap<Row>>(kRowShards);
   size_t size() const {
     size_t n = 0;
     for (const auto& m : shard) n += m.size();
     return n;
   }
   Row& operator[](uint64_t key) { return shard[row_shard(key)][key]; }
-  const Row* find(uint64_t key) const {
-    const auto& m = shard[row_shard(key)];
-    const auto it = m.find(key);
-    return it == m.end() ? nullptr : &it->second;
-  }
+  const Row* find(uint64_t key) const { return shard[row_shard(key)].find(key); }
   std::vector<uint64_t> sorted_keys() const {
     std::vector<uint64_t> ks;
     ks.reserve(size());
-    for (const auto& m : shard)
-      for (const auto& kv : m) ks.push_back(kv.first);
+    for (const auto& m : shard) m.each([&](uint64_t k, const Row&) { ks.push_back(k); });
     std::sort(ks.begin(), ks.end());
     return ks;
   }
@@ -504,7 +550,7 @@ struct Ctx {
   uint32_t t;       // traversal index
   uint32_t launch;  // (iteration-1)*N + player
   int rb;
-  std::unordered_map<uint64_t, Acc>* acc;  // this thread's accumulators, one map per row shard
+  FlatMap<Acc>* acc;  // this thread's accumulators, one map per row shard
   Counters* cnt;
   mccfr_trace* trace;
   float w;
@@ -1003,8 +1049,7 @@ static int step(Oracle& O, long long iteration, int player, int batch, mccfr_tra
   const float w = R.c.use_linear_cfr ? (float)iteration : 1.0f;
   if (nthreads < 1) nthreads = 1;
   if (O.float_mode) nthreads = 1;
-  std::vector<std::vector<std::unordered_map<uint64_t, Acc>>> accs(
-      nthreads, std::vector<std::unordered_map<uint64_t, Acc>>(kRowShards));
+  std::vector<std::vector<FlatMap<Acc>>> accs(nthreads, std::vector<FlatMap<Acc>>(kRowShards));
   std::vector<Counters> cnts(nthreads);
   // Float mode keeps per-row FP32 sums in traversal order, so it runs on one thread.
   std::atomic<int> next{0};
@@ -1039,10 +1084,9 @@ static int step(Oracle& O, long long iteration, int player, int batch, mccfr_tra
   // the CFR+ clamp sweep (cfr_gpu.cu:1018-1022) over the rows this update touched.
   const double sr = std::ldexp(1.0, -rb);
   const double ss = std::ldexp(1.0, -32);
-  auto apply = [&](std::unordered_map<uint64_t, Row>& rows, const std::unordered_map<uint64_t, Acc>& all) {
-    for (const auto& kv : all) {
-      Row& row = rows[kv.first];
-      const Acc& A = kv.second;
+  auto apply = [&](FlatMap<Row>& rows, const FlatMap<Acc>& all) {
+    all.each([&](uint64_t key, const Acc& A) {
+      Row& row = rows[key];
       for (int a = 0; a < 8; ++a) {
         float r;
         float s;
@@ -1058,7 +1102,7 @@ static int step(Oracle& O, long long iteration, int player, int batch, mccfr_tra
         row.s[a] = s;
       }
       row.visits += A.visits;
-    }
+    });
   };
   std::atomic<int> next_shard{0};
   auto fold = [&]() {
@@ -1067,18 +1111,18 @@ static int step(Oracle& O, long long iteration, int player, int batch, mccfr_tra
         apply(O.rows.shard[sh], accs[0][sh]);
         continue;
       }
-      std::unordered_map<uint64_t, Acc> all;
+      FlatMap<Acc> all;
       for (auto& per_thread : accs)
-        for (const auto& kv : per_thread[sh]) {
-          Acc& A = all[kv.first];
+        per_thread[sh].each([&](uint64_t key, const Acc& src) {
+          Acc& A = all[key];
           for (int a = 0; a < 8; ++a) {
-            A.dr[a] += kv.second.dr[a];
-            A.ds[a] += kv.second.ds[a];
-            A.fr[a] += kv.second.fr[a];
-            A.fs[a] += kv.second.fs[a];
+            A.dr[a] += src.dr[a];
+            A.ds[a] += src.ds[a];
+            A.fr[a] += src.fr[a];
+            A.fs[a] += src.fs[a];
           }
-          A.visits += kv.second.visits;
-        }
+          A.visits += src.visits;
+        });
       apply(O.rows.shard[sh], all);
     }
   };
