@@ -88,3 +88,22 @@ def test_regret_fraction_bits():
     # batch * 64 visits * 20 * N * stack * 2^rb must stay below 2^61
     assert 8 <= rb <= 24
     assert (1 << 20) * 64 * 20 * 6 * 10000 * (1 << rb) < (1 << 63)
+
+
+def test_thread_count_does_not_change_rows(hand_table):
+    """The oracle sums each update's deltas in integers and folds rows shard by
+    shard, so its rows are the same on one thread and on eight."""
+    L = mccfr.lib
+    for preset, batch, players in ((L.PRESET_6MAX_100BB, 64, 6), (L.PRESET_REF8, 2048, 2)):
+        cfg = L.preset(preset)
+        rows = []
+        for threads in (1, 8):
+            o = binding.Oracle(cfg, hand_table)
+            for it in (1, 2):
+                for p in range(players):
+                    o.step(it, p, batch, threads=threads)
+            rows.append(o.export_rows())
+            o.close()
+        for f in ("keys", "visits", "regrets", "strategy_sum"):
+            assert np.array_equal(np.asarray(rows[0][f]).view(np.uint8), np.asarray(rows[1][f]).view(np.uint8)), f
+        assert rows[0]["keys"].size > 0
