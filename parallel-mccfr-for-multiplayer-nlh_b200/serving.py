@@ -285,7 +285,14 @@ def poisson_arrivals(rng: np.random.Generator, n: int, rate: float) -> np.ndarra
 
 
 def summarize(results: list[Result]) -> dict:
-    lat = np.array([r.latency_ms for r in results])
-    span = max(r.finished for r in results) - min(r.arrival for r in results)
-    return {"requests": len(results), "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "mean_ms": float(lat.mean()), "solves_per_s": len(results) / span}
+    """Latency percentiles and throughput of the solved requests; cancelled ones
+    are counted apart."""
+    done = [r for r in results if not r.cancelled]
+    out = {"requests": len(done), "cancelled": len(results) - len(done)}
+    if not done:
+        return out
+    lat = np.array([r.latency_ms for r in done])
+    span = max(r.finished for r in done) - min(r.arrival for r in done)
+    out.update({"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                "mean_ms": float(lat.mean()), "solves_per_s": len(done) / span if span > 0 else None})
+    return out

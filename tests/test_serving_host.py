@@ -4,6 +4,7 @@ from __future__ import annotations
 import importlib
 
 import numpy as np
+import pytest
 
 from conftest import mccfr  # noqa: F401  (registers mccfr_b200)
 
@@ -174,3 +175,13 @@ def test_cancel_from_another_thread_is_safe():
     th.join()
     assert res[reqs[2].rid].cancelled  # still queued behind the single slot when withdrawn
     assert not res[reqs[0].rid].cancelled and not res[reqs[1].rid].cancelled
+
+
+def test_summary_leaves_out_cancelled_requests():
+    e = (np.zeros(0, np.uint32), np.zeros((0, 8), np.float32))
+    res = [sv.Result(0, 0.0, 0.0, 0.1, *e), sv.Result(1, 0.0, 0.0, 0.3, *e),
+           sv.Result(2, 0.0, 0.0, 9.0, *e, cancelled=True)]
+    s = sv.summarize(res)
+    assert s["requests"] == 2 and s["cancelled"] == 1
+    assert s["p50_ms"] == pytest.approx(200.0) and s["mean_ms"] == pytest.approx(200.0)
+    assert sv.summarize(res[2:]) == {"requests": 0, "cancelled": 1}
