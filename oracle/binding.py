@@ -35,6 +35,8 @@ def lib() -> ctypes.CDLL:
         o.orc_destroy.argtypes = [c_void_p]
         o.orc_set_float_mode.argtypes = [c_void_p, c_int]
         o.orc_step.argtypes = [c_void_p, c_longlong, c_int, c_int, c_void_p, c_int]
+        o.orc_step_wave.argtypes = [c_void_p, c_longlong, c_int, c_int, c_int]
+        o.orc_wave_hist.argtypes = [c_void_p, c_void_p, c_int]
         o.orc_train.argtypes = [c_void_p, c_longlong, c_int, c_int]
         o.orc_counters.argtypes = [c_void_p, c_void_p]
         o.orc_export_rows.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, POINTER(c_size_t)]
@@ -99,6 +101,17 @@ class Oracle:
         buf = np.zeros(batch, dtype=trace_dtype) if trace else None
         lib().orc_step(self._h, iteration, player, batch, _p(buf) if trace else None, threads)
         return buf
+
+    def step_wave(self, iteration: int, player: int, batch: int, threads: int = 8) -> int:
+        """The same player-update, expanded level by level (orc_step_wave);
+        returns the status (integer-sum mode only)."""
+        return lib().orc_step_wave(self._h, iteration, player, batch, threads)
+
+    def wave_hist(self) -> np.ndarray:
+        """Nodes per tree depth in the last level-synchronous update."""
+        out = np.zeros(512, np.int64)
+        n = lib().orc_wave_hist(self._h, _p(out), out.size)
+        return out[: min(n, out.size)]
 
     def train(self, iters: int, batch: int, threads: int = 8):
         lib().orc_train(self._h, iters, batch, threads)

@@ -523,6 +523,9 @@ struct Oracle {
   bool float_mode = false;
   int64_t iterations_done = 0;
   Counters total;
+  // level-synchronous updates: nodes per depth, summed over traversals
+  std::vector<int64_t> wave_hist;
+  std::mutex wave_mu;
 };
 
 // Fixed-point fraction bits of a player-update's regret deltas: chosen so that
@@ -554,6 +557,7 @@ struct Ctx {
   Counters* cnt;
   mccfr_trace* trace;
   float w;
+  Game* root_out = nullptr;  // set: build the traversal's root game here instead of walking it
 };
 
 static inline const Row* find_row(const Oracle& O, uint64_t key) { return O.rows.find(key); }
@@ -934,6 +938,10 @@ static void run_subgame_traversal(Ctx& C) {
   g.n_to_act = 0;
   for (int i = 1; i <= N; ++i) g.to_act[g.n_to_act++] = (g.dealer + i) % N;
   C.cnt->T++;
+  if (C.root_out) {
+    *C.root_out = g;
+    return;
+  }
   traverse(C, g, 0);
 }
 
@@ -1036,12 +1044,197 @@ static void run_traversal(Ctx& C) {
     }
   }
   C.cnt->T++;
+  if (C.root_out) {
+    *C.root_out = g;
+    return;
+  }
   const float v = traverse(C, g, 0);
   if (C.trace) C.trace->payoff = v;
 }
 
+
+// ---------------------------------------------------------------------------
+// Level-synchronous form of the same update (a prototype of a breadth-first
+// device traversal): the traversals of a chunk are expanded together, one tree
+// level at a time, then their values return level by level.  Every node is one
+// call of traverse() above, with the same arithmetic in the same order, so the
+// rows equal the depth-first walk's bit for bit (deltas are summed in integers,
+// draws are keyed by the node's path).
+// ---------------------------------------------------------------------------
+struct WNode {
+  Game g;
+  uint32_t t = 0;
+  int kind = 0;   // 0 terminal, 1 one child passes its value up, 2 updating player (all
+                  // legal actions), 3 updating player (one sampled action)
+  int first = 0;  // first child in the next level
+  int s = 0;
+  uint8_t vm = 0;
+  float q = 0.0f, value = 0.0f;
+  uint64_t key = 0;
+  float strat[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+};
+
+// traverse() up to the point where it would recurse: the node gets its kind,
+// its value if terminal, and its children appended to `next`.
+static void wave_expand(Ctx& C, WNode& n, int depth, std::vector<WNode>& next) {
+  const Oracle& O = *C.O;
+  const Rules& R = O.R;
+  Game& g = n.g;
+  auto push = [&](const Game& ch) {
+    WNode c;
+    c.g = ch;
+    c.t = n.t;
+    next.push_back(c);
+  };
+  if (depth >= R.c.max_depth) {
+    C.cnt->X++;
+    n.value = 0.0f;
+    return;
+  }
+  int active = 0, winner = -1;
+  for (int i = 0; i < g.N; ++i)
+    if (!(g.folded & (1u << i))) {
+      active++;
+      winner = i;
+    }
+  if (active == 1) {
+    C.cnt->X++;
+    n.value = (winner == C.up) ? (float)(g.pot - g.inv[C.up]) : (float)(-g.inv[C.up]);
+    return;
+  }
+  if (g.n_to_act == 0) {
+    if (g.street < 3) {
+      g.street++;
+      for (int i = 0; i < g.N; ++i) g.bets[i] = 0;
+      g.cb = 0;
+      g.lfr = R.c.big_blind;
+      g.raises = 0;
+      g.n_to_act = 0;
+      for (int i = 1; i <= g.N; ++i) {
+        const int p = (g.dealer + i) % g.N;
+        if (!(g.folded & (1u << p)) && !(g.all_in & (1u << p))) g.to_act[g.n_to_act++] = p;
+      }
+      if (g.n_to_act > 0) {
+        n.kind = 1;
+        n.first = (int)next.size();
+        push(g);
+        return;
+      }
+    }
+    C.cnt->X++;
+    n.value = showdown(g, C.up);
+    return;
+  }
+  const int player = g.to_act[0];
+  const int to_call = g.cb - g.bets[player];
+  const uint8_t vm = valid_mask(R, g.pot, g.stacks[player], to_call, g.cb, g.lfr, g.raises);
+  const uint64_t key = info_key(O, g, player);
+  const Row* row = find_row(O, key);
+  static const float zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const float* reg = row ? row->r : zero;
+  C.cnt->V++;
+  const U4 draw = philox(U4{n.t, C.launch, (uint32_t)g.path, (uint32_t)(g.path >> 32) | 0x80000000u},
+                         (uint32_t)R.c.seed, (uint32_t)(R.c.seed >> 32));
+  const float u = uniform01(draw.x);
+  auto child_of = [&](int a, Game& ch) {
+    ch = g;
+    ch.n_to_act--;
+    for (int i = 0; i < ch.n_to_act; ++i) ch.to_act[i] = ch.to_act[i + 1];
+    if (apply_action(R, ch, player, a)) rebuild_queue(ch, player);
+  };
+  n.first = (int)next.size();
+  if (player == C.up) {
+    node_strategy(reg, vm, n.strat);
+    C.cnt->U++;
+    n.key = key;
+    n.vm = vm;
+    if (R.c.sampling == MCCFR_SAMPLING_REFERENCE) {
+      n.s = sample_action(R, reg, vm, u);
+      n.q = std::fmax(n.strat[n.s], 0.05f);
+      Game ch;
+      child_of(n.s, ch);
+      push(ch);
+      n.kind = 3;
+      return;
+    }
+    for (int a = 0; a < 8; ++a) {
+      if (!(vm & (1u << a))) continue;
+      Game ch;
+      child_of(a, ch);
+      push(ch);
+    }
+    n.kind = 2;
+    return;
+  }
+  const int s = sample_action(R, reg, vm, u);
+  if (R.c.sampling == MCCFR_SAMPLING_EXTERNAL) {
+    float strat[8];
+    node_strategy(reg, vm, strat);
+    record_node(C, key, vm, nullptr, strat, false, true);
+  }
+  Game ch;
+  child_of(s, ch);
+  push(ch);
+  n.kind = 1;
+}
+
+// Traversals [t0, t1) of one player-update, level by level.
+static void run_wave(Ctx& C, uint32_t t0, uint32_t t1, std::vector<int64_t>& hist) {
+  std::vector<std::vector<WNode>> level(1);
+  for (uint32_t t = t0; t < t1; ++t) {
+    WNode n;
+    n.t = t;
+    C.t = t;
+    C.root_out = &n.g;
+    run_traversal(C);  // deal, buckets and blinds: the root game
+    C.root_out = nullptr;
+    level[0].push_back(n);
+  }
+  for (size_t d = 0; !level[d].empty(); ++d) {
+    std::vector<WNode> next;
+    for (WNode& n : level[d]) wave_expand(C, n, (int)d, next);
+    if (hist.size() <= d) hist.resize(d + 1, 0);
+    hist[d] += (int64_t)level[d].size();
+    level.push_back(std::move(next));
+  }
+  for (size_t d = level.size() - 1; d-- > 0;) {
+    const std::vector<WNode>& below = level[d + 1];
+    for (WNode& n : level[d]) {
+      if (n.kind == 1) {
+        n.value = below[n.first].value;
+      } else if (n.kind == 2) {  // the same sums as traverse()'s external-sampling branch
+        float v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        int c = n.first;
+        for (int a = 0; a < 8; ++a)
+          if (n.vm & (1u << a)) v[a] = below[c++].value;
+        float vh = 0.0f;
+        for (int a = 0; a < 8; ++a)
+          if (n.vm & (1u << a)) vh = vh + n.strat[a] * v[a];
+        Acc& A = C.acc[row_shard(n.key)][n.key];
+        A.visits++;
+        const int64_t fvh = fix_r(vh, C.rb);
+        for (int a = 0; a < 8; ++a) {
+          if (!(n.vm & (1u << a))) continue;
+          A.dr[a] += fix_r(v[a], C.rb) - fvh;
+          A.fr[a] += v[a] - vh;
+        }
+        n.value = vh;
+      } else if (n.kind == 3) {  // traverse()'s reference-rule branch
+        const float child = below[n.first].value;
+        float rd[8];
+        for (int a = 0; a < 8; ++a) rd[a] = ((a == n.s) ? (child / n.q) : 0.0f) - child;
+        record_node(C, n.key, n.vm, rd, n.strat, true, true);
+        n.value = child;
+      }
+    }
+  }
+}
+
 static int step(Oracle& O, long long iteration, int player, int batch, mccfr_trace* trace,
-                int nthreads) {
+                int nthreads, bool wave = false) {
+  // the level-synchronous form keeps integer sums only (float mode sums FP32 in
+  // depth-first order) and writes no per-path traces
+  if (wave && (O.float_mode || trace)) return MCCFR_ERR_INVALID_ARG;
   const Rules& R = O.R;
   const int N = R.c.num_players;
   const uint32_t launch = (uint32_t)((iteration - 1) * N + player);
@@ -1053,11 +1246,17 @@ static int step(Oracle& O, long long iteration, int player, int batch, mccfr_tra
   std::vector<Counters> cnts(nthreads);
   // Float mode keeps per-row FP32 sums in traversal order, so it runs on one thread.
   std::atomic<int> next{0};
+  std::vector<std::vector<int64_t>> hists(nthreads);
   auto worker = [&](int tid) {
     for (;;) {
       const int b = next.fetch_add(32);
       if (b >= batch) break;
       const int e = std::min(batch, b + 32);
+      if (wave) {
+        Ctx C{&O, player, (uint32_t)b, launch, rb, accs[tid].data(), &cnts[tid], nullptr, w};
+        run_wave(C, (uint32_t)b, (uint32_t)e, hists[tid]);
+        continue;
+      }
       for (int t = b; t < e; ++t) {
         Ctx C{&O, player, (uint32_t)t, launch, rb, accs[tid].data(), &cnts[tid],
               trace ? &trace[t] : nullptr, w};
@@ -1071,6 +1270,14 @@ static int step(Oracle& O, long long iteration, int player, int batch, mccfr_tra
     std::vector<std::thread> th;
     for (int i = 0; i < nthreads; ++i) th.emplace_back(worker, i);
     for (auto& x : th) x.join();
+  }
+  if (wave) {
+    std::lock_guard<std::mutex> lock(O.wave_mu);
+    O.wave_hist.clear();
+    for (const auto& h : hists) {
+      if (O.wave_hist.size() < h.size()) O.wave_hist.resize(h.size(), 0);
+      for (size_t d = 0; d < h.size(); ++d) O.wave_hist[d] += h[d];
+    }
   }
   for (auto& c : cnts) {
     O.total.V += c.V;
@@ -1209,6 +1416,21 @@ void orc_set_float_mode(void* h, int on) { ((Oracle*)h)->float_mode = on != 0; }
 
 int orc_step(void* h, long long iteration, int player, int batch, mccfr_trace* trace, int nthreads) {
   return step(*(Oracle*)h, iteration, player, batch, trace, nthreads);
+}
+
+// The same player-update in the level-synchronous form (integer sums, no traces).
+int orc_step_wave(void* h, long long iteration, int player, int batch, int nthreads) {
+  return step(*(Oracle*)h, iteration, player, batch, nullptr, nthreads, true);
+}
+
+// Nodes per tree depth in the last level-synchronous update, summed over its
+// traversals; returns the number of depths (at most `cap` are written).
+int orc_wave_hist(void* h, int64_t* out, int cap) {
+  Oracle& O = *(Oracle*)h;
+  std::lock_guard<std::mutex> lock(O.wave_mu);
+  const int n = (int)O.wave_hist.size();
+  for (int d = 0; d < n && d < cap; ++d) out[d] = O.wave_hist[d];
+  return n;
 }
 
 int orc_train(void* h, long long iters, int batch, int nthreads) {
