@@ -231,7 +231,9 @@ int mccfr_load_checkpoint(mccfr_handle* h, const char* path);
    resumed from it equals uninterrupted training bit for bit.  Loading replaces
    the table's contents and the iteration count; it refuses a file written for a
    different game or abstraction (every config field but device and table_log2)
-   and keys that cannot belong to this table. */
+   and keys that cannot belong to this table.  A subgame's board, pot and ranges
+   are not in the file: load a subgame checkpoint into a handle created for the
+   same subgame. */
 int mccfr_save_checkpoint_v2(mccfr_handle* h, const char* path);
 int mccfr_load_checkpoint_v2(mccfr_handle* h, const char* path);
 /* Strategy dump v2: [u64 0x53545241540100][u32 2^26][u32 8][u32 n]{u32 key, f32[8]}. */
