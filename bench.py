@@ -629,42 +629,58 @@ def main():
 
     tr.close()
     if rank == 0 and world == 1 and not args.no_extras:
+        # secondary measurements: one that fails is recorded as its error, the
+        # headline figures above are kept either way
         extras = {}
-        extras["batched_same_table"] = batched_same_table(m, L, table, args, value)
-        extras["c3_multitable"] = multitable(m, L, table)
-        extras["resolve_serving"] = serving_sweep(m, L, table)
-        extras["hu_subgame_exploitability"] = hu_subgame_exploitability(m, L, table)
-        extras["c4_showdown"] = c4_showdown(m, L, table)
-        for wl in ("ref8-6max", "6max-100bb-refrule"):
-            if wl == args.workload:
-                continue
+
+        def extra(name, fn):
+            try:
+                extras[name] = fn()
+            except Exception as e:  # noqa: BLE001
+                extras[name] = {"error": f"{type(e).__name__}: {e}"}
+
+        def refrule_rate(wl):
             c2, b2 = make_config(L, wl)
             t2 = m.GPUCFRTrainer(config=c2)
-            t2.set_hand_table(table)
-            t2.train(3, b2, verbose=False)
-            a0 = t2.stats()
-            st2 = torch.cuda.ExternalStream(t2.stream_ptr(), device=local_rank)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(st2)
-            t2.train(5, b2, verbose=False, timed=True)
-            e1.record(st2)
-            e1.synchronize()
-            a1 = t2.stats()
-            ms2 = e0.elapsed_time(e1)
-            n2 = a1.traversals - a0.traversals
-            extras[wl] = {"traversals_per_s": n2 / (ms2 / 1e3), "batch": b2, "iterations": 5,
-                          "traverse_kernel_ms": (a1.traverse_ms - a0.traverse_ms) / (5 * c2.num_players),
-                          "apply_kernel_ms": (a1.apply_ms - a0.apply_ms) / (5 * c2.num_players)}
-            t2.close()
+            try:
+                t2.set_hand_table(table)
+                t2.train(3, b2, verbose=False)
+                a0 = t2.stats()
+                st2 = torch.cuda.ExternalStream(t2.stream_ptr(), device=local_rank)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st2)
+                t2.train(5, b2, verbose=False, timed=True)
+                e1.record(st2)
+                e1.synchronize()
+                a1 = t2.stats()
+                ms2 = e0.elapsed_time(e1)
+                n2 = a1.traversals - a0.traversals
+                return {"traversals_per_s": n2 / (ms2 / 1e3), "batch": b2, "iterations": 5,
+                        "traverse_kernel_ms": (a1.traverse_ms - a0.traverse_ms) / (5 * c2.num_players),
+                        "apply_kernel_ms": (a1.apply_ms - a0.apply_ms) / (5 * c2.num_players)}
+            finally:
+                t2.close()
+
+        extra("batched_same_table", lambda: batched_same_table(m, L, table, args, value))
+        extra("c3_multitable", lambda: multitable(m, L, table))
+        extra("resolve_serving", lambda: serving_sweep(m, L, table))
+        extra("hu_subgame_exploitability", lambda: hu_subgame_exploitability(m, L, table))
+        extra("c4_showdown", lambda: c4_showdown(m, L, table))
+        for wl in ("ref8-6max", "6max-100bb-refrule"):
+            if wl != args.workload:
+                extra(wl, lambda wl=wl: refrule_rate(wl))
         out["extras"] = extras
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sample = {"6max-100bb": 16384, "6max-100bb-refrule": 65536, "hu-20bb": 16384}.get(args.workload, 65536)
         vpt = visits / max(1, trav)  # this run's timed iterations
-        rate, info = cpu_traversal_rate(L, cfg, sample, vpt)
-        out["cpu_baseline"] = {"value": rate, "unit": "traversals/s", "cores": info["cores"], "kind": "port",
-                               "sample": cpu_sample_text(sample, info, vpt),
-                               "raw_traversals_per_s": info["raw_traversals_per_s"]}
+        try:
+            rate, info = cpu_traversal_rate(L, cfg, sample, vpt)
+            out["cpu_baseline"] = {"value": rate, "unit": "traversals/s", "cores": info["cores"], "kind": "port",
+                                   "sample": cpu_sample_text(sample, info, vpt),
+                                   "raw_traversals_per_s": info["raw_traversals_per_s"]}
+        except Exception as e:  # noqa: BLE001
+            out["cpu_baseline"] = {"value": None, "unit": "traversals/s", "error": f"{type(e).__name__}: {e}"}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
