@@ -37,6 +37,7 @@ def lib() -> ctypes.CDLL:
         o.orc_step.argtypes = [c_void_p, c_longlong, c_int, c_int, c_void_p, c_int]
         o.orc_step_wave.argtypes = [c_void_p, c_longlong, c_int, c_int, c_int]
         o.orc_wave_hist.argtypes = [c_void_p, c_void_p, c_int]
+        o.orc_showdown_masks.argtypes = [c_void_p, c_longlong, c_int, c_int, c_void_p]
         o.orc_train.argtypes = [c_void_p, c_longlong, c_int, c_int]
         o.orc_counters.argtypes = [c_void_p, c_void_p]
         o.orc_export_rows.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, POINTER(c_size_t)]
@@ -106,6 +107,13 @@ class Oracle:
         """The same player-update, expanded level by level (orc_step_wave);
         returns the status (integer-sum mode only)."""
         return lib().orc_step_wave(self._h, iteration, player, batch, threads)
+
+    def showdown_masks(self, iteration: int, player: int, n: int) -> np.ndarray:
+        """Winner masks (bit q: seat q holds the best rank) of the deals of
+        traversals 0..n-1 of update (iteration, player)."""
+        out = np.zeros(n, np.uint8)
+        assert lib().orc_showdown_masks(self._h, iteration, player, n, _p(out)) == 0
+        return out
 
     def wave_hist(self) -> np.ndarray:
         """Nodes per tree depth in the last level-synchronous update."""

@@ -1423,6 +1423,32 @@ int orc_step_wave(void* h, long long iteration, int player, int batch, int nthre
   return step(*(Oracle*)h, iteration, player, batch, nullptr, nthreads, true);
 }
 
+// Showdown winners of the deals of traversals 0..n-1 of update (iteration,
+// player), the deals training uses (cfr_gpu.cu:460-470, 942-952): bit q of
+// masks[t] is set when seat q holds the best 7-card rank (several bits: a
+// split).  Every seat is live, as in a checked-down pot.
+int orc_showdown_masks(void* h, long long iteration, int player, int n, uint8_t* masks) {
+  Oracle& O = *(Oracle*)h;
+  if (O.sg.street) return MCCFR_ERR_INVALID_ARG;
+  const int N = O.R.c.num_players;
+  const uint32_t launch = (uint32_t)((iteration - 1) * N + player);
+  FlatMap<Acc> unused[kRowShards];
+  Counters cnt;
+  for (int t = 0; t < n; ++t) {
+    Game g;
+    Ctx C{&O, player, (uint32_t)t, launch, 8, unused, &cnt, nullptr, 1.0f};
+    C.root_out = &g;
+    run_traversal(C);
+    uint16_t best = 0;
+    for (int q = 0; q < g.N; ++q) best = std::max(best, g.river_rank[q]);
+    uint8_t m = 0;
+    for (int q = 0; q < g.N; ++q)
+      if (g.river_rank[q] == best) m |= (uint8_t)(1u << q);
+    masks[t] = m;
+  }
+  return 0;
+}
+
 // Nodes per tree depth in the last level-synchronous update, summed over its
 // traversals; returns the number of depths (at most `cap` are written).
 int orc_wave_hist(void* h, int64_t* out, int cap) {

@@ -107,3 +107,28 @@ def test_thread_count_does_not_change_rows(hand_table):
         for f in ("keys", "visits", "regrets", "strategy_sum"):
             assert np.array_equal(np.asarray(rows[0][f]).view(np.uint8), np.asarray(rows[1][f]).view(np.uint8)), f
         assert rows[0]["keys"].size > 0
+
+
+def test_showdown_masks_match_the_dealt_hands(hand_table):
+    """orc_showdown_masks (the checker for a 6-seat showdown microbench) equals
+    winners recomputed from the dealt cards that a traced update records, and
+    the seats win evenly."""
+    L = mccfr.lib
+    cfg = L.preset(L.PRESET_6MAX_100BB)
+    cfg.sampling, cfg.max_depth = L.SAMPLING_REFERENCE, 64  # traces exist for the reference rule
+    o = binding.Oracle(cfg, hand_table)
+    n = 4096
+    masks = o.showdown_masks(1, 0, n)
+    tr = o.step(1, 0, n, trace=True, trace_dtype=L.TRACE_DTYPE)  # the same deals
+    cards = np.concatenate([tr["hole"].reshape(n, 6, 2), np.repeat(tr["board"][:, None, :], 6, axis=1)], axis=2)
+    ranks = binding.eval7(hand_table, cards.reshape(-1, 7).astype(np.uint8)).reshape(n, 6)
+    want = ((ranks == ranks.max(axis=1, keepdims=True)) * (1 << np.arange(6))).sum(axis=1)
+    assert np.array_equal(masks, want.astype(np.uint8))
+    big = o.showdown_masks(2, 3, 60000)
+    assert np.all((big > 0) & (big < 64))
+    wins = np.array([((big >> q) & 1).sum() for q in range(6)])
+    expect = wins.mean()
+    assert np.all(np.abs(wins - expect) < 5 * np.sqrt(expect))
+    split = np.mean([bin(int(x)).count("1") > 1 for x in big])
+    assert 0.0 < split < 0.2
+    o.close()
