@@ -58,6 +58,9 @@ def parse():
                     help="only: train heads-up 20BB for ITERS iterations with each update rule and print the "
                          "exact best-response exploitability of both (a long run; one JSON line)")
     ap.add_argument("--br-flop-stride", type=int, default=1, help="with --hu-exploitability: flop-class stride")
+    ap.add_argument("--curve", type=str, default="", metavar="I1,I2,...",
+                    help="only: time single iterations at these points of one training run (one JSON line)")
+    ap.add_argument("--form", type=int, default=-1, help="traversal form (0 auto, 1 lanes, 2 levels)")
     return ap.parse_args()
 
 
@@ -183,51 +186,147 @@ def profiled_traffic(workload: str) -> dict | None:
         return None
 
 
-def cpu_traversal_rate(L, cfg, batch_sample: int, visits_per_traversal: float | None = None) -> tuple[float, dict]:
-    """The oracle (the reference path's C++ restatement) on host cores, timed on
-    one player-update of `batch_sample` traversals from an empty table.
-
-    A traversal's cost depends on the training state: from an empty table every
-    strategy is uniform and a 6-max traversal visits about 1,000 decision nodes,
-    where the GPU's timed iterations visit about 55.  Given the node visits per
-    traversal of the iterations being compared, the rate is returned in
-    traversals of that size: the oracle's node visits per second divided by it.
-    The raw figures stay in the info dict."""
+def _binding():
     sys.path.insert(0, str(ROOT / "oracle"))
     import binding
 
+    return binding
+
+
+def cpu_equal_work(rows: dict, cfg, iterations_done: int, batch: int, table, sample: int) -> dict:
+    """The oracle (the reference path's C++ restatement) on all host cores, on
+    exactly the trees the device walks next: the device's rows after
+    `iterations_done` iterations are loaded into the oracle, which then runs
+    traversals 0..sample-1 of update (iterations_done + 1, player 0), the same
+    deals, draws and table reads as the device's first `sample` traversals of that
+    update.  Returns traversals/s with the work per traversal it saw."""
+    binding = _binding()
     threads = os.cpu_count() or 1
-    table = L.hand_table()
     orc = binding.Oracle(cfg, table)
     t0 = time.perf_counter()
-    orc.step(1, 0, batch_sample, threads=threads)
+    orc.import_rows(rows, iterations_done)
+    load_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    orc.step(iterations_done + 1, 0, sample, threads=threads)
     dt = time.perf_counter() - t0
-    visits = orc.counters()["visits"]
+    c = orc.counters()
     orc.close()
-    info = {"cores": threads, "seconds": dt, "raw_traversals_per_s": batch_sample / dt,
-            "visits_per_traversal": visits / batch_sample, "visits_per_s": visits / dt}
-    if visits_per_traversal:
-        return visits / dt / visits_per_traversal, info
-    return batch_sample / dt, info
+    return {"value": sample / dt, "unit": "traversals/s", "cores": threads, "kind": "port",
+            "seconds": dt, "rows_loaded": int(rows["keys"].size), "load_seconds": load_s,
+            "V_per_traversal": c["visits"] / sample, "U_per_traversal": c["updates"] / sample,
+            "sample": (f"traversals 0..{sample - 1} of update (iteration {iterations_done + 1}, player 0) of the "
+                       f"{batch}-traversal workload, on the device's {int(rows['keys'].size)} rows after iteration "
+                       f"{iterations_done} loaded into the oracle: the trees the device walks next "
+                       f"({c['visits'] / sample:.1f} node visits per traversal), {dt:.1f} s on {threads} threads, "
+                       "update and fold included")}
 
 
-def work_per_traversal(workload: str) -> float | None:
-    """Decision-node visits per traversal of the bench's timed iterations on this
-    workload, measured on the GPU (profiles/work_per_traversal.json)."""
+# Traversals per player-update of the reference arm's own training run: a batch
+# the CPU port trains through in seconds per iteration on the host's cores.
+REFERENCE_ARM_BATCH = {"6max-100bb": 4096, "6max-100bb-refrule": 65536, "hu-20bb": 16384, "hu-20bb-refrule": 65536,
+                       "ref8-6max": 65536, "ref8-hu": 65536}
+
+
+def repo_libraries() -> list[str]:
+    """Shared libraries of this repository mapped into the process
+    (/proc/self/maps), relative to the repository root."""
+    out = set()
     try:
-        d = json.loads((ROOT / "profiles" / "work_per_traversal.json").read_text())
-        return float(d[workload]["visits_per_traversal"])
-    except Exception:
-        return None
+        for line in Path("/proc/self/maps").read_text().splitlines():
+            parts = line.split()
+            if len(parts) >= 6 and parts[-1].endswith(".so") and parts[-1].startswith(str(ROOT)):
+                out.add(os.path.relpath(parts[-1], ROOT))
+    except OSError:
+        pass
+    return sorted(out)
 
 
-def cpu_sample_text(sample: int, info: dict, v: float | None) -> str:
-    head = (f"{sample} traversals of one player-update from an empty table (iteration 1, player 0), "
-            f"{info['seconds']:.1f} s on {info['cores']} threads: {info['visits_per_traversal']:.0f} node visits "
-            f"per traversal, {info['visits_per_s']:.3g} visits/s, {info['raw_traversals_per_s']:.0f} raw traversals/s")
-    if v:
-        return head + f"; value = visits/s / {v:.2f} visits per traversal of the GPU's timed iterations"
-    return head + "; value = raw traversals/s (no GPU visit count recorded for this workload)"
+def reference_arm(args, workload: str, world: int) -> dict:
+    """The reference path's CPU implementation (the oracle, all host threads)
+    training the workload's game from an empty table by itself: W iterations,
+    then K timed iterations, each of N player-updates of a bounded batch.  It
+    loads no device library: presets and the rank table come from the oracle."""
+    import importlib
+
+    binding = _binding()
+    L = importlib.import_module("mccfr_b200.lib")  # struct definitions only; libmccfr.so is not loaded
+    preset_name, over, batch = WORKLOADS[workload]
+    cfg = binding.config_init(L.Config(), getattr(L, preset_name))
+    for k, v in over.items():
+        setattr(cfg, k, v)
+    if args.table_log2:
+        cfg.table_log2 = args.table_log2
+    if args.key_bits >= 0:
+        cfg.key_bits = args.key_bits
+    b = args.batch or REFERENCE_ARM_BATCH.get(workload, 4096)
+    threads = os.cpu_count() or 1
+    table = binding.hand_table()
+    orc = binding.Oracle(cfg, table)
+    orc.train(args.warmup, b, threads=threads)
+    c0 = orc.counters()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        orc.train(1, b, threads=threads)
+    secs = time.perf_counter() - t0
+    c1 = orc.counters()
+    orc.close()
+    trav = c1["traversals"] - c0["traversals"]
+    v = trav / secs
+    vpt = (c1["visits"] - c0["visits"]) / max(1, trav)
+    upt = (c1["updates"] - c0["updates"]) / max(1, trav)
+    metric = "6-max traversals/s" if cfg.num_players == 6 else "traversals/s"
+    sample = (f"the oracle training the workload's game by itself from an empty table on {threads} threads: "
+              f"{args.warmup} warm-up iterations, then {args.steps} timed iterations of {cfg.num_players} "
+              f"player-updates x {b} traversals (iterations {args.warmup + 1}-{args.warmup + args.steps}); "
+              f"{vpt:.1f} node visits and {upt:.2f} updating-player updates per traversal. Its trees are those "
+              f"of a {b}-traversal run, larger than the device's at {batch} traversals per update (the device "
+              "line's cpu_baseline times the oracle on the device's own trees)")
+    return {
+        "impl": "reference", "metric": metric, "value": v, "unit": "traversals/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / max(1, args.steps),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": describe(cfg, workload, batch),
+        "cpu_baseline": {"value": v, "unit": "traversals/s", "cores": threads, "kind": "port", "sample": sample,
+                         "V_per_traversal": vpt, "U_per_traversal": upt, "traversals_per_update": b},
+        "e2e": {"value": v, "unit": "traversals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "libraries_loaded": repo_libraries(),
+    }
+
+
+def iteration_curve(m, L, table, cfg, batch: int, points: list[int]) -> dict:
+    """Traversals/s and work per traversal of single iterations along one
+    training run of a fresh table: iteration i is timed alone (CUDA events on
+    the trainer's stream) after iterations 1..i-1 ran untimed."""
+    import torch
+
+    tr = m.GPUCFRTrainer(config=cfg)
+    tr.set_hand_table(table)
+    stream = torch.cuda.ExternalStream(tr.stream_ptr())
+    out, done = [], 0
+    t_start = time.perf_counter()
+    for it in sorted(set(points)):
+        if it - 1 > done:
+            tr.train(it - 1 - done, batch, verbose=False)
+            done = it - 1
+        s0 = tr.stats()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        tr.train(1, batch, verbose=False, timed=True)
+        e1.record(stream)
+        e1.synchronize()
+        done = it
+        s1 = tr.stats()
+        ms = e0.elapsed_time(e1)
+        n = s1.traversals - s0.traversals
+        out.append({"iteration": it, "traversals_per_s": n / (ms / 1e3), "ms": ms,
+                    "V_per_traversal": (s1.node_visits - s0.node_visits) / n,
+                    "U_per_traversal": (s1.traverser_updates - s0.traverser_updates) / n,
+                    "traverse_ms_per_update": (s1.traverse_ms - s0.traverse_ms) / cfg.num_players,
+                    "apply_ms_per_update": (s1.apply_ms - s0.apply_ms) / cfg.num_players,
+                    "touched_rows_last_update": int(s1.touched_last)})
+    tr.close()
+    return {"points": out, "wall_s": time.perf_counter() - t_start, "traversals_per_update": batch,
+            "form": int(cfg.traversal_form)}
 
 
 def batched_same_table(m, L, table, args, plain_value) -> dict:
@@ -497,6 +596,15 @@ def main():
 
     import __graft_entry__ as ge
 
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        # the checker libraries only: this arm loads no product library
+        ge._build_module().build_oracle()
+        ge.load_package()
+        print(json.dumps(reference_arm(args, args.workload, world)), flush=True)
+        return
+
     ge.build()
     m = ge.load_package()
     L = m.lib
@@ -507,35 +615,9 @@ def main():
         cfg.table_log2 = args.table_log2
     if args.key_bits >= 0:
         cfg.key_bits = args.key_bits
+    if args.form >= 0:
+        cfg.traversal_form = args.form
     metric = "6-max traversals/s" if cfg.num_players == 6 else "traversals/s"
-
-    if args.impl == "reference":
-        if rank != 0:
-            return
-        # bounded per-step samples of the same workload on all host cores
-        sample = {"6max-100bb": 16384, "6max-100bb-refrule": 65536, "hu-20bb": 16384}.get(args.workload, 65536)
-        vpt = work_per_traversal(args.workload)
-        for _ in range(args.warmup):
-            cpu_traversal_rate(L, cfg, max(64, sample // 8), vpt)
-        rates, secs = [], 0.0
-        cores = os.cpu_count() or 1
-        info = {}
-        for _ in range(args.steps):
-            r, info = cpu_traversal_rate(L, cfg, sample, vpt)
-            rates.append(r)
-            secs += info["seconds"]
-            cores = info["cores"]
-        v = statistics.median(rates)
-        desc = "per step: " + cpu_sample_text(sample, info, vpt)
-        print(json.dumps({
-            "impl": "reference", "metric": metric, "value": v, "unit": "traversals/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / max(1, args.steps),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": describe(cfg, args.workload, batch),
-            "cpu_baseline": {"value": v, "unit": "traversals/s", "cores": cores, "kind": "port", "sample": desc},
-            "e2e": {"value": v, "unit": "traversals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        }), flush=True)
-        return
 
     import torch
     import torch.distributed as dist
@@ -547,6 +629,12 @@ def main():
         dist.init_process_group(backend, timeout=timedelta(seconds=300))
     cfg.device = local_rank
     table = L.hand_table()
+    if args.curve:
+        if rank == 0:
+            pts = [int(x) for x in args.curve.split(",") if x.strip()]
+            print(json.dumps({"workload": args.workload, **iteration_curve(m, L, table, cfg, batch, pts)}),
+                  flush=True)
+        return
     if args.hu_exploitability:
         if rank == 0:
             print(json.dumps(hu_full_exploitability(m, L, table, args.hu_exploitability, args.br_flop_stride)),
@@ -578,6 +666,16 @@ def main():
     updates = s1.traverser_updates - s0.traverser_updates
     launches = args.steps * cfg.num_players
     trav_ms = s1.traverse_ms - s0.traverse_ms
+
+    # the table after the timed region: the oracle's CPU baseline walks the same
+    # trees as the device's next update (taken before the e2e steps run it)
+    cpu_rows = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu_rows = tr.export_rows()
+        except Exception as e:  # noqa: BLE001
+            cpu_rows = e
+    cpu_iterations = args.warmup + args.steps
 
     # e2e through the C ABI: host call per step, schedule H2D inside, stats D2H read
     t0 = time.perf_counter()
@@ -631,13 +729,21 @@ def main():
     if rank == 0 and world == 1 and not args.no_extras:
         # secondary measurements: one that fails is recorded as its error, the
         # headline figures above are kept either way
+        # secondary measurements after a CUDA error would run on a poisoned
+        # context: the first such error is recorded and the rest are skipped
         extras = {}
+        poisoned = []
 
         def extra(name, fn):
+            if poisoned:
+                extras[name] = {"skipped": f"a CUDA error in {poisoned[0]} came first"}
+                return
             try:
                 extras[name] = fn()
             except Exception as e:  # noqa: BLE001
                 extras[name] = {"error": f"{type(e).__name__}: {e}"}
+                if getattr(e, "status", None) == 2 or "CUDA" in str(e):
+                    poisoned.append(name)
 
         def refrule_rate(wl):
             c2, b2 = make_config(L, wl)
@@ -672,15 +778,14 @@ def main():
         out["extras"] = extras
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sample = {"6max-100bb": 16384, "6max-100bb-refrule": 65536, "hu-20bb": 16384}.get(args.workload, 65536)
-        vpt = visits / max(1, trav)  # this run's timed iterations
         try:
-            rate, info = cpu_traversal_rate(L, cfg, sample, vpt)
-            out["cpu_baseline"] = {"value": rate, "unit": "traversals/s", "cores": info["cores"], "kind": "port",
-                                   "sample": cpu_sample_text(sample, info, vpt),
-                                   "raw_traversals_per_s": info["raw_traversals_per_s"]}
+            if isinstance(cpu_rows, Exception):
+                raise cpu_rows
+            out["cpu_baseline"] = cpu_equal_work(cpu_rows, cfg, cpu_iterations, batch, table,
+                                                 min(batch, 1 << 20))
         except Exception as e:  # noqa: BLE001
             out["cpu_baseline"] = {"value": None, "unit": "traversals/s", "error": f"{type(e).__name__}: {e}"}
+        cpu_rows = None
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:

@@ -114,8 +114,30 @@ typedef struct mccfr_config {
      table_log2 >= 26), key k owns row k-1 and lookups never probe; otherwise
      the table is open-addressed.  Results are the same either way. */
   int32_t key_bits;
-  int32_t reserved[7];
+  /* External sampling only: how the traversal kernel walks the updating player's
+     tree (MCCFR_FORM_*).  Every form gives bit-identical tables, so this field is
+     not part of the game (a v2 checkpoint loads into any form). */
+  int32_t traversal_form;
+  /* MCCFR_FORM_LEVELS only: capacity of the updating-player node buffer as
+     log2 of the node records (80 B each; the child buffer holds four times as
+     many 12 B entries); 0 = sized from the batch.  Subtrees that do not fit are
+     walked depth first inside the same update, with the same result. */
+  int32_t level_log2;
+  int32_t reserved[5];
 } mccfr_config;
+
+/* Traversal forms (external sampling). */
+enum {
+  MCCFR_FORM_AUTO = 0,   /* the level-synchronous form */
+  /* one lane per traversal, depth first, with an explicit frame stack
+     (persistent lanes pulling traversals from a work counter) */
+  MCCFR_FORM_LANES = 1,
+  /* level-synchronous: all traversals of the update advance together, one
+     level of the updating player's decisions per launch (the opponents'
+     sampled actions between two of its decisions are walked within the level),
+     then the values return level by level */
+  MCCFR_FORM_LEVELS = 2
+};
 
 /* Counters and timings of one handle. */
 typedef struct mccfr_stats {
@@ -212,6 +234,12 @@ int mccfr_num_info_sets_active(mccfr_handle* h, long long* out);
 int mccfr_export_rows(mccfr_handle* h, uint64_t* keys, float* regrets,
                       float* strategy_sum, uint64_t* visits, size_t capacity,
                       size_t* count);
+/* Order-independent checksum of every occupied row, computed on the device
+   without copying rows out: the sum (mod 2^64) over rows of a 64-bit mix of the
+   row's key, the bits of its regrets and strategy sums, and its update count.
+   Two tables with the same rows have the same digest; *rows receives the
+   occupied-row count.  No reference counterpart (a test and monitoring aid). */
+int mccfr_table_digest(mccfr_handle* h, uint64_t* digest, uint64_t* rows);
 /* Dense SoA [8][2^26] tables of the reference (FNV26 mode only). */
 int mccfr_export_tables(mccfr_handle* h, float* regrets, float* strategy_sum,
                         size_t n);

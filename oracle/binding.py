@@ -41,6 +41,10 @@ def lib() -> ctypes.CDLL:
         o.orc_train.argtypes = [c_void_p, c_longlong, c_int, c_int]
         o.orc_counters.argtypes = [c_void_p, c_void_p]
         o.orc_export_rows.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, POINTER(c_size_t)]
+        o.orc_table_digest.argtypes = [c_void_p, c_void_p, c_void_p]
+        o.orc_config_init.argtypes = [c_void_p, c_int]
+        o.orc_hand_table_generate.argtypes = [c_void_p, c_size_t]
+        o.orc_import_rows.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_longlong]
         o.orc_get_strategy.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, POINTER(c_size_t)]
         o.orc_philox.argtypes = [c_void_p, c_void_p, c_void_p]
         o.orc_uniform01.restype = c_float
@@ -140,6 +144,26 @@ class Oracle:
         lib().orc_export_rows(self._h, _p(keys), _p(reg), _p(ssum), _p(vis), m, ctypes.byref(n))
         return {"keys": keys, "regrets": reg, "strategy_sum": ssum, "visits": vis}
 
+    def digest(self) -> tuple[int, int]:
+        """(checksum, rows) of the table, the figures mccfr_table_digest gives
+        for a device table with the same rows."""
+        out = np.zeros(2, np.uint64)
+        assert lib().orc_table_digest(self._h, _p(out[:1]), _p(out[1:])) == 0
+        return int(out[0]), int(out[1])
+
+    def import_rows(self, rows: dict, iterations_done: int = 0) -> None:
+        """Replaces the table with `rows` (the dict export_rows returns, e.g. a
+        device trainer's export) and sets the completed-iteration count."""
+        keys = np.ascontiguousarray(rows["keys"], dtype=np.uint64)
+        reg = np.ascontiguousarray(rows["regrets"], dtype=np.float32).reshape(-1, 8)
+        ssum = np.ascontiguousarray(rows["strategy_sum"], dtype=np.float32).reshape(-1, 8)
+        vis = np.ascontiguousarray(rows["visits"], dtype=np.uint64)
+        n = keys.size
+        assert reg.shape[0] == ssum.shape[0] == vis.size == n
+        rc = lib().orc_import_rows(self._h, _p(keys), _p(reg), _p(ssum), _p(vis), n, iterations_done)
+        if rc:
+            raise ValueError(f"orc_import_rows: status {rc}")
+
     def strategy_arrays(self):
         n = c_size_t()
         lib().orc_get_strategy(self._h, None, None, None, 0, ctypes.byref(n))
@@ -148,6 +172,27 @@ class Oracle:
         probs = np.empty((m, 8), np.float32)
         lib().orc_get_strategy(self._h, _p(keys), None, _p(probs), m, ctypes.byref(n))
         return keys[: n.value], probs[: n.value]
+
+
+def config_init(cfg, preset: int):
+    """Fills a config struct (the ctypes mirror of mccfr_config) with one of the
+    three presets, without the device library."""
+    rc = lib().orc_config_init(ctypes.byref(cfg), int(preset))
+    if rc:
+        raise ValueError(f"orc_config_init: status {rc}")
+    return cfg
+
+
+HAND_TABLE_ENTRIES = 32487834
+
+
+def hand_table() -> np.ndarray:
+    """The 32,487,834-entry rank table, built on the host by the oracle library."""
+    t = np.empty(HAND_TABLE_ENTRIES, dtype=np.int32)
+    rc = lib().orc_hand_table_generate(_p(t), t.size)
+    if rc:
+        raise RuntimeError(f"orc_hand_table_generate: status {rc}")
+    return t
 
 
 def philox(ctr, key) -> np.ndarray:

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "../include/mccfr.h"
+#include "../parallel-mccfr-for-multiplayer-nlh_b200/csrc/handtable.h"
 
 namespace orc {
 
@@ -1428,9 +1429,11 @@ int orc_step_wave(void* h, long long iteration, int player, int batch, int nthre
 // masks[t] is set when seat q holds the best 7-card rank (several bits: a
 // split).  Every seat is live, as in a checked-down pot.
 int orc_showdown_masks(void* h, long long iteration, int player, int n, uint8_t* masks) {
+  if (!h || n < 0 || (n > 0 && !masks) || iteration < 1) return MCCFR_ERR_INVALID_ARG;
   Oracle& O = *(Oracle*)h;
   if (O.sg.street) return MCCFR_ERR_INVALID_ARG;
   const int N = O.R.c.num_players;
+  if (player < 0 || player >= N) return MCCFR_ERR_INVALID_ARG;
   const uint32_t launch = (uint32_t)((iteration - 1) * N + player);
   FlatMap<Acc> unused[kRowShards];
   Counters cnt;
@@ -1466,6 +1469,144 @@ int orc_train(void* h, long long iters, int batch, int nthreads) {
     for (int p = 0; p < O.R.c.num_players; ++p) step(O, it, p, batch, nullptr, nthreads);
     O.iterations_done = it;
   }
+  return 0;
+}
+
+// The three workload presets as plain values (the same games mccfr_config_init
+// describes), so that a CPU-only run needs no device library: the reference's
+// constructor defaults and 8-slot abstraction (cfr_gpu.cuh:50-55,
+// abstraction.h:9-10, 42-53), heads-up 20BB and 6-max 100BB.
+// The rank table the reference's evaluator reads from a file, built on the host
+// (the generator of this project's product library, compiled into the oracle so
+// that CPU-only runs need no device library).
+int orc_hand_table_generate(int32_t* out, size_t n) {
+  if (!out || n < (size_t)MCCFR_HAND_TABLE_ENTRIES) return MCCFR_ERR_INVALID_ARG;
+  int states = 0;
+  return mccfr::generate_hand_table(out, n, &states) == (int64_t)MCCFR_HAND_TABLE_ENTRIES ? 0 : MCCFR_ERR_FORMAT;
+}
+
+int orc_config_init(mccfr_config* c, int preset) {
+  if (!c) return MCCFR_ERR_INVALID_ARG;
+  std::memset(c, 0, sizeof(*c));
+  c->use_cfr_plus = 1;
+  c->use_linear_cfr = 1;
+  if (preset == MCCFR_PRESET_REF8) {
+    c->num_players = 2;
+    c->starting_stack = 1000;
+    c->small_blind = 10;
+    c->big_blind = 20;
+    c->sampling = MCCFR_SAMPLING_REFERENCE;
+    c->key_mode = MCCFR_KEY_FNV26;
+    c->num_actions = 8;
+    const int kinds[8] = {MCCFR_ACT_FOLD, MCCFR_ACT_CHECK, MCCFR_ACT_CALL, MCCFR_ACT_RAISE_MIN,
+                          MCCFR_ACT_RAISE_POT, MCCFR_ACT_RAISE_POT, MCCFR_ACT_RAISE_POT, MCCFR_ACT_ALL_IN};
+    const int nums[8] = {0, 0, 0, 0, 1, 2, 1, 0}, dens[8] = {1, 1, 1, 1, 2, 3, 1, 1};
+    for (int a = 0; a < 8; ++a) {
+      c->action_kind[a] = kinds[a];
+      c->action_num[a] = nums[a];
+      c->action_den[a] = dens[a];
+    }
+    c->max_depth = 20;
+    c->preflop_mode = MCCFR_PREFLOP_CHEN64;
+    c->preflop_buckets = 64;
+    c->postflop_mode = MCCFR_POSTFLOP_REF_LINEAR;
+    c->postflop_buckets[0] = c->postflop_buckets[1] = c->postflop_buckets[2] = 128;
+    c->table_log2 = 26;
+    c->seed = 42;
+    return 0;
+  }
+  if (preset != MCCFR_PRESET_HU_20BB && preset != MCCFR_PRESET_6MAX_100BB) return MCCFR_ERR_INVALID_ARG;
+  const bool hu = preset == MCCFR_PRESET_HU_20BB;
+  c->num_players = hu ? 2 : 6;
+  c->small_blind = 50;
+  c->big_blind = 100;
+  c->starting_stack = hu ? 2000 : 10000;
+  c->sampling = MCCFR_SAMPLING_EXTERNAL;
+  c->key_mode = MCCFR_KEY_ID64;
+  if (hu) {
+    const int kinds[4] = {MCCFR_ACT_FOLD, MCCFR_ACT_CHECK_CALL, MCCFR_ACT_RAISE_POT, MCCFR_ACT_ALL_IN};
+    c->num_actions = 4;
+    for (int a = 0; a < 4; ++a) {
+      c->action_kind[a] = kinds[a];
+      c->action_num[a] = 1;
+      c->action_den[a] = 1;
+    }
+    c->raise_cap = 2;
+    c->postflop_buckets[0] = c->postflop_buckets[1] = c->postflop_buckets[2] = 50;
+    c->seed = 0;
+  } else {
+    const int kinds[6] = {MCCFR_ACT_FOLD, MCCFR_ACT_CHECK_CALL, MCCFR_ACT_RAISE_POT,
+                          MCCFR_ACT_RAISE_POT, MCCFR_ACT_RAISE_POT, MCCFR_ACT_ALL_IN};
+    const int nums[6] = {0, 0, 1, 1, 2, 0}, dens[6] = {1, 1, 2, 1, 1, 1};
+    c->num_actions = 6;
+    for (int a = 0; a < 6; ++a) {
+      c->action_kind[a] = kinds[a];
+      c->action_num[a] = nums[a];
+      c->action_den[a] = dens[a];
+    }
+    c->raise_cap = 3;
+    c->postflop_buckets[0] = c->postflop_buckets[1] = c->postflop_buckets[2] = 200;
+    c->seed = 1;
+  }
+  c->max_depth = 255;
+  c->preflop_mode = MCCFR_PREFLOP_CLASS169;
+  c->preflop_buckets = 169;
+  c->postflop_mode = MCCFR_POSTFLOP_RANK_CDF;
+  c->key_bits = 26;
+  c->table_log2 = 27;
+  return 0;
+}
+
+// Replaces every row with the n given rows (regrets, strategy sums and visit
+// counts per key) and sets the completed-iteration count: a table state handed
+// over from another trainer, e.g. a device trainer's export, so that the next
+// player-update walks exactly the trees that trainer's next update walks.
+int orc_import_rows(void* h, const uint64_t* keys, const float* R, const float* S, const uint64_t* visits,
+                    size_t n, long long iterations_done) {
+  if (!h || (n && (!keys || !R || !S || !visits)) || iterations_done < 0) return MCCFR_ERR_INVALID_ARG;
+  Oracle& O = *(Oracle*)h;
+  for (size_t i = 0; i < n; ++i)
+    if (keys[i] == 0) return MCCFR_ERR_INVALID_ARG;
+  O.rows = RowTable();
+  for (size_t i = 0; i < n; ++i) {
+    Row& r = O.rows[keys[i]];
+    std::memcpy(r.r, R + 8 * i, 32);
+    std::memcpy(r.s, S + 8 * i, 32);
+    r.visits = visits[i];
+  }
+  O.iterations_done = iterations_done;
+  return 0;
+}
+
+// The checksum mccfr_table_digest computes on the device, over the oracle's
+// rows: sum (mod 2^64) of a 64-bit mix of each row's key, value bits and update
+// count, in this fixed mixing order.
+static uint64_t row_digest(uint64_t key, const float* reg, const float* ssum, uint64_t visits) {
+  uint64_t h = mix64(key ^ 0x9E3779B97F4A7C15ull);
+  for (int a = 0; a < 8; ++a) {
+    uint32_t b;
+    std::memcpy(&b, reg + a, 4);
+    h = mix64(h ^ (uint64_t)b ^ ((uint64_t)a << 32));
+  }
+  for (int a = 0; a < 8; ++a) {
+    uint32_t b;
+    std::memcpy(&b, ssum + a, 4);
+    h = mix64(h ^ (uint64_t)b ^ ((uint64_t)(a + 8) << 32));
+  }
+  return mix64(h ^ visits);
+}
+
+int orc_table_digest(void* h, uint64_t* digest, uint64_t* rows) {
+  if (!h || !digest) return MCCFR_ERR_INVALID_ARG;
+  Oracle& O = *(Oracle*)h;
+  uint64_t sum = 0, n = 0;
+  for (const auto& m : O.rows.shard)
+    m.each([&](uint64_t k, const Row& r) {
+      sum += row_digest(k, r.r, r.s, r.visits);
+      n++;
+    });
+  *digest = sum;
+  if (rows) *rows = n;
   return 0;
 }
 

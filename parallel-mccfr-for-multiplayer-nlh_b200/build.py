@@ -18,10 +18,10 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libmccfr.so"
 ORACLE_DIR = ROOT / "oracle"
-REFERENCE_SRC = Path("/root/reference/poker_cuda/src")
 
 SOURCES = ["mccfr.cu", "eval_static.cu", "best_response.cu", "handtable.cpp", "abstraction.cpp"]
-HEADERS = ["game.cuh", "table.cuh", "traverse_ref.cuh", "traverse_es.cuh", "batched.cuh", "handtable.h", "best_response.h"]
+HEADERS = ["game.cuh", "table.cuh", "traverse_ref.cuh", "traverse_es.cuh", "traverse_levels.cuh", "batched.cuh",
+           "handtable.h", "best_response.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -73,11 +73,18 @@ def build_cli(force: bool = False) -> Path:
     return CLI
 
 
+def reference_sources_present() -> bool:
+    """Whether oracle/Makefile finds the reference's sources (its REF directory,
+    MCCFR_REFERENCE_SRC when set)."""
+    r = subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), "ref-check"], capture_output=True, text=True)
+    return r.returncode == 0 and r.stdout.strip() == "yes"
+
+
 def build_oracle(force: bool = False) -> Path:
     """Builds oracle/liboracle.so and, when the reference sources are present,
     oracle/_ref/libref.so (test infrastructure only)."""
     targets = ["all"]
-    if REFERENCE_SRC.exists():
+    if reference_sources_present():
         targets.append("ref")
     cmd = ["make", "-s", "-C", str(ORACLE_DIR)]
     if force:

@@ -79,6 +79,16 @@ __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
   return z;
 }
 
+// Checksum term of one table row (mccfr_table_digest): the row's key, the bits
+// of its regrets and strategy sums and its update count, mixed in a fixed order.
+__host__ __device__ __forceinline__ uint64_t row_digest(uint64_t key, const uint32_t* reg_bits,
+                                                        const uint32_t* ssum_bits, uint64_t visits) {
+  uint64_t h = mix64(key ^ 0x9E3779B97F4A7C15ull);
+  for (int a = 0; a < 8; ++a) h = mix64(h ^ (uint64_t)reg_bits[a] ^ ((uint64_t)a << 32));
+  for (int a = 0; a < 8; ++a) h = mix64(h ^ (uint64_t)ssum_bits[a] ^ ((uint64_t)(a + 8) << 32));
+  return mix64(h ^ visits);
+}
+
 // ---------------------------------------------------------------------------
 // Rank table helpers (cfr_gpu.cu:87-112).
 // ---------------------------------------------------------------------------

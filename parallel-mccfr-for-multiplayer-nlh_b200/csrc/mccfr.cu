@@ -31,6 +31,7 @@
 #include "table.cuh"
 #include "traverse_ref.cuh"
 #include "traverse_es.cuh"
+#include "traverse_levels.cuh"
 #include "batched.cuh"
 #include "best_response.h"
 
@@ -148,6 +149,35 @@ __global__ void k_count_rows(const TableView tv, unsigned long long cap_slots, u
     c += *row_key(tv, s) != 0;
   c = __reduce_add_sync(0xFFFFFFFFu, c);
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(on, c);
+}
+
+// Order-independent digest of the occupied rows (mccfr_table_digest).
+__global__ void k_digest(const TableView tv, unsigned long long cap_slots, unsigned long long* __restrict__ out) {
+  unsigned long long sum = 0, rows = 0;
+  for (unsigned long long s = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; s < cap_slots;
+       s += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long k = *row_key(tv, s);
+    if (!k) continue;
+    const uint32_t* r = reinterpret_cast<const uint32_t*>(row_reg(tv, s));
+    const uint32_t* q = reinterpret_cast<const uint32_t*>(row_ssum(tv, s));
+    uint32_t rb[8], qb[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      rb[a] = r[a];
+      qb[a] = q[a];
+    }
+    sum += row_digest(k, rb, qb, *row_visits(tv, s));
+    rows++;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sum += __shfl_down_sync(0xFFFFFFFFu, sum, o);
+    rows += __shfl_down_sync(0xFFFFFFFFu, rows, o);
+  }
+  if ((threadIdx.x & 31) == 0 && rows) {
+    atomicAdd(out, sum);
+    atomicAdd(out + 1, rows);
+  }
 }
 
 // Compacts the occupied rows into arrays of `bound` rows (unordered).
@@ -318,6 +348,12 @@ struct mccfr_handle {
   Sched* h_sched = nullptr;  // pinned
   Counters* d_counters = nullptr;
   unsigned* d_work = nullptr;  // traversal work counter of the persistent kernel
+  // level-synchronous form: node and seed buffers of one update
+  void* d_level = nullptr;
+  size_t level_bytes = 0;
+  int level_batch = 0;  // batch the buffers were sized for
+  LevelBufs lb{};
+  int grid_expand = 0, grid_back = 0, grid_dfs = 0;  // resident blocks on this handle's device
   // graph of one iteration
   cudaGraphExec_t graph = nullptr;
   int graph_batch = -1;
@@ -402,6 +438,10 @@ int validate(const mccfr_config& c, std::string& why) {
     if (c.postflop_buckets[s] < 1 || c.postflop_buckets[s] > 256) return why = "postflop buckets must be 1..256", 1;
   if (c.table_log2 < 10 || c.table_log2 > 31) return why = "table_log2 must be 10..31", 1;
   if (c.key_bits < 0 || c.key_bits > 48) return why = "key_bits must be 0..48", 1;
+  if (c.traversal_form < MCCFR_FORM_AUTO || c.traversal_form > MCCFR_FORM_LEVELS)
+    return why = "unknown traversal form", 1;
+  if (c.level_log2 != 0 && (c.level_log2 < 8 || c.level_log2 > 30))
+    return why = "level_log2 must be 0 or 8..30", 1;
   // Reference rule walks one path; its records hold the updating player's nodes.
   if (c.sampling == MCCFR_SAMPLING_REFERENCE && c.raise_cap == 0 && c.max_depth > 2 * kMaxRec)
     return why = "reference sampling without a raise cap needs max_depth <= 48", 1;
@@ -495,6 +535,9 @@ int record(mccfr_handle* h, cudaEvent_t e, bool capturing) {
   return MCCFR_OK;
 }
 
+bool use_levels(const mccfr_handle* h);
+int enqueue_levels(mccfr_handle* h, int batch, float rscale);
+
 // Enqueues one player-update (traverse + apply) reading the device schedule;
 // `ev3` (optional) receives event records before, between and after.
 int enqueue_update(mccfr_handle* h, int batch, mccfr_trace* d_trace, cudaEvent_t* ev3, bool capturing = false) {
@@ -514,14 +557,132 @@ int enqueue_update(mccfr_handle* h, int batch, mccfr_trace* d_trace, cudaEvent_t
     else
       k_traverse_ref<kRefBlock, false><<<grid, kRefBlock, 0, h->stream>>>(h->gp, h->tv, h->d_deals, h->d_sched,
                                                                             batch, rscale, h->d_counters, nullptr);
+  } else if (use_levels(h)) {
+    const int rc = enqueue_levels(h, batch, rscale);
+    if (rc) return rc;
   } else {
-    launch_traverse_es(h->gp, h->tv, h->d_deals, h->d_sched, batch, rscale, h->d_counters, h->d_work, h->stream);
+    launch_traverse_es(h->gp, h->tv, h->d_deals, h->d_sched, batch, rscale, h->d_counters, h->d_work, h->stream,
+                       h->device);
   }
   CK(cudaGetLastError());
   if (ev3 && record(h, ev3[1], capturing)) return MCCFR_ERR_CUDA;
   k_apply<<<148 * 8, 256, 0, h->stream>>>(h->gp, h->tv, h->d_sched, rinv);
   CK(cudaGetLastError());
   if (ev3 && record(h, ev3[2], capturing)) return MCCFR_ERR_CUDA;
+  return MCCFR_OK;
+}
+
+// Traversal form of the update: the level-synchronous kernels for external
+// sampling unless the config asks for the depth-first lanes.
+bool use_levels(const mccfr_handle* h) {
+  return h->cfg.sampling == MCCFR_SAMPLING_EXTERNAL && h->cfg.traversal_form != MCCFR_FORM_LANES;
+}
+
+// Seed levels of an update: the updating player acts at most raise_cap + 1
+// times per street (once, and once more after each raise of another player),
+// and at most once per node of the depth cut; one more level holds the seeds
+// below its last possible decision.  Capped at kMaxLevels (the deepest level
+// is then walked depth first).
+int level_count(const mccfr_handle* h) {
+  const mccfr_config& c = h->cfg;
+  const int streets = h->gp.sub_street ? 4 - h->gp.sub_street : 4;
+  int decisions = c.max_depth;
+  if (c.raise_cap > 0) decisions = std::min(decisions, streets * (c.raise_cap + 1));
+  return std::min(decisions + 1, kMaxLevels);
+}
+
+// Node and seed buffers for updates of `batch` traversals: 2^level_log2 node
+// records (default: 64 per traversal, 2^18..2^26) and 8 seeds per node (at
+// least the batch and a margin).  A smaller allocation is tried when the
+// device is short of memory; any size gives the same rows.
+int ensure_levels(mccfr_handle* h, int batch) {
+  const int nlev = level_count(h);
+  if (h->d_level && h->level_batch >= batch) {
+    if (h->lb.nlev != nlev && h->graph) {  // a subgame re-targeted to another street
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+      h->graph_batch = -1;
+    }
+    h->lb.nlev = nlev;
+    return MCCFR_OK;
+  }
+  if (h->d_level) {
+    CK(cudaStreamSynchronize(h->stream));
+    cudaFree(h->d_level);
+    h->d_level = nullptr;
+    h->level_batch = 0;
+  }
+  int lg = h->cfg.level_log2;
+  if (!lg) {
+    lg = 18;
+    while (lg < 26 && (1ull << lg) < 64ull * (unsigned long long)batch) ++lg;
+  }
+  for (;; --lg) {
+    const unsigned long long nodes = 1ull << lg;
+    const unsigned long long seeds = std::max(8ull * nodes, (unsigned long long)batch + (1ull << 20));
+    const size_t bytes = nodes * (sizeof(EsState) + sizeof(uint4)) + seeds * 12 + sizeof(LevelCtl) + 256;
+    const cudaError_t e = cudaMalloc(&h->d_level, bytes);
+    if (e == cudaSuccess) {
+      char* p = static_cast<char*>(h->d_level);
+      h->lb.nodes = reinterpret_cast<EsState*>(p);
+      p += nodes * sizeof(EsState);
+      h->lb.meta = reinterpret_cast<uint4*>(p);
+      p += nodes * sizeof(uint4);
+      h->lb.child = reinterpret_cast<uint32_t*>(p);
+      p += seeds * 4;
+      h->lb.cstrat = reinterpret_cast<float*>(p);
+      p += seeds * 4;
+      h->lb.value = reinterpret_cast<float*>(p);
+      p += seeds * 4;
+      h->lb.ctl = reinterpret_cast<LevelCtl*>(p);
+      h->lb.node_cap = (uint32_t)nodes;
+      h->lb.seed_cap = (uint32_t)seeds;
+      h->level_bytes = bytes;
+      h->level_batch = batch;
+      break;
+    }
+    cudaGetLastError();  // clear the allocation error
+    if (e != cudaErrorMemoryAllocation || lg <= 12)
+      return fail(h, MCCFR_ERR_OOM, "level buffers: %s", cudaGetErrorString(e));
+  }
+  h->lb.nlev = nlev;
+  if (!h->grid_expand) {
+    int sms = 0, per = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_level_expand<128, 1>, 128, 0));
+    h->grid_expand = std::max(1, per) * sms;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_level_back<256>, 256, 0));
+    h->grid_back = std::max(1, per) * sms;
+    const size_t smem = 2 * 128 * sizeof(EsFrame);
+    CK(cudaFuncSetAttribute(k_level_dfs<128, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_level_dfs<128, 2, 1>, 128, smem));
+    h->grid_dfs = std::max(1, per) * sms;
+  }
+  if (h->graph) {  // the graph captured the old buffers
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+    h->graph_batch = -1;
+  }
+  return MCCFR_OK;
+}
+
+// One external-sampling update in the level-synchronous form: the levels
+// expanded top down, the seeds that did not fit walked depth first, the values
+// returned bottom up.
+int enqueue_levels(mccfr_handle* h, int batch, float rscale) {
+  const LevelBufs& lb = h->lb;
+  CK(cudaMemsetAsync(lb.ctl, 0, sizeof(LevelCtl), h->stream));
+  for (int L = 0; L < lb.nlev; ++L)
+    k_level_expand<128, 1><<<h->grid_expand, 128, 0, h->stream>>>(h->gp, h->tv, h->d_deals, h->d_sched, batch, lb,
+                                                                  L, h->d_counters);
+  CK(cudaGetLastError());
+  k_level_dfs<128, 2, 1><<<h->grid_dfs, 128, 2 * 128 * sizeof(EsFrame), h->stream>>>(
+      h->gp, h->tv, h->d_deals, h->d_sched, batch, rscale, lb, h->d_counters);
+  CK(cudaGetLastError());
+  for (int L = lb.nlev - 2; L >= 0; --L)
+    k_level_back<256><<<h->grid_back, 256, 0, h->stream>>>(h->gp, h->tv, h->d_sched, batch, rscale, lb, L,
+                                                           h->d_counters);
+  CK(cudaGetLastError());
   return MCCFR_OK;
 }
 
@@ -545,7 +706,8 @@ int ensure_deals(mccfr_handle* h, int batch) {
 
 int ensure_graph(mccfr_handle* h, int batch) {
   {
-    const int rc = ensure_deals(h, batch);
+    int rc = ensure_deals(h, batch);
+    if (!rc && use_levels(h)) rc = ensure_levels(h, batch);
     if (rc) return rc;
   }
   if (h->graph && h->graph_batch == batch) return MCCFR_OK;
@@ -697,6 +859,7 @@ void release(mccfr_handle* h) {
   cudaFreeHost(h->h_sched);
   cudaFree(h->d_counters);
   cudaFree(h->d_work);
+  cudaFree(h->d_level);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -1014,6 +1177,7 @@ int mccfr_step(mccfr_handle* h, long long iteration, int player, int batch, mccf
     CK(cudaMemsetAsync(d_trace, 0, (size_t)batch * sizeof(mccfr_trace), h->stream));
   }
   int rc = ensure_deals(h, batch);
+  if (rc == MCCFR_OK && use_levels(h)) rc = ensure_levels(h, batch);
   if (rc == MCCFR_OK) rc = set_sched(h, iteration, player);
   if (rc == MCCFR_OK) rc = enqueue_update(h, batch, d_trace, h->ev);
   if (rc == MCCFR_OK) {
@@ -1127,6 +1291,26 @@ int mccfr_get_stats(mccfr_handle* h, mccfr_stats* out) {
   out->device_error = h->sticky_err;
   out->touched_last = h->touched_last;
   out->rows_used = -1;  // filled by mccfr_export_rows callers; counting needs a table scan
+  return MCCFR_OK;
+}
+
+int mccfr_table_digest(mccfr_handle* h, uint64_t* digest, uint64_t* rows) {
+  if (!h || !digest) return MCCFR_ERR_INVALID_ARG;
+  CK(cudaSetDevice(h->device));
+  unsigned long long* d = nullptr;
+  CK(cudaMalloc(&d, 2 * sizeof(unsigned long long)));
+  unsigned long long out[2] = {0, 0};
+  cudaError_t e = cudaMemsetAsync(d, 0, sizeof(out), h->stream);
+  if (e == cudaSuccess) {
+    k_digest<<<148 * 16, 256, 0, h->stream>>>(h->tv, h->cap, d);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, sizeof(out), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(h, MCCFR_ERR_CUDA, "digest: %s", cudaGetErrorString(e));
+  *digest = out[0];
+  if (rows) *rows = out[1];
   return MCCFR_OK;
 }
 
@@ -1314,11 +1498,13 @@ int mccfr_load_checkpoint(mccfr_handle* h, const char* path) {
 namespace {
 constexpr uint64_t kCkptV2Magic = 0x324B43524643434DULL;  // "MCCFRCK2" little-endian
 
-// The fields that define the game and its abstraction: all but the device and
-// the table capacity.
+// The fields that define the game and its abstraction: all but the device, the
+// table capacity and the traversal form (every form gives the same tables).
 bool same_game(mccfr_config a, mccfr_config b) {
   a.device = b.device = 0;
   a.table_log2 = b.table_log2 = 0;
+  a.traversal_form = b.traversal_form = 0;
+  a.level_log2 = b.level_log2 = 0;
   std::memset(a.reserved, 0, sizeof(a.reserved));
   std::memset(b.reserved, 0, sizeof(b.reserved));
   return std::memcmp(&a, &b, sizeof(a)) == 0;

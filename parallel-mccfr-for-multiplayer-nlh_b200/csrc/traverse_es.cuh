@@ -29,9 +29,11 @@ struct EsState {
   int cb, lfr;
   uint32_t q;        // action queue, 4-bit entries
   uint32_t abits;
+  uint32_t aux;      // traversal index (the level-synchronous form keeps states apart from their lanes)
   uint64_t path;
   uint8_t folded, allin, street, raises, nq, depth, pad0, pad1;
 };
+static_assert(sizeof(EsState) == 64, "a betting state is one 64-byte record");
 
 // Chips behind of `player`: everyone starts with G.stack behind and, in a
 // subgame, an equal share of the dead pot already invested.
@@ -125,6 +127,7 @@ __device__ __forceinline__ void es_begin(const GameParams& G, const DealRec* D, 
   L.sp = 0;
   L.value = 0.0f;
   L.ret = false;
+  L.cur.aux = t;
   if (G.sub_street) {
     // subgame: the dead pot split equally, everyone with the same stack, first
     // to act after the dealer (the last seat)
@@ -415,19 +418,24 @@ k_traverse_es(const GameParams G, const TableView tv, const DealRec* __restrict_
 // The two shallowest frames of each walk live in shared memory (measured best
 // among 0-4 staged frames and probe widths 1-2 on both presets).
 inline void launch_traverse_es(const GameParams& G, const TableView& tv, const DealRec* deals, const Sched* sched,
-                               int batch, float rscale, Counters* counters, unsigned* work, cudaStream_t stream) {
+                               int batch, float rscale, Counters* counters, unsigned* work, cudaStream_t stream,
+                               int device) {
   constexpr int B = 128, K = 2;
   constexpr size_t smem = (size_t)K * B * sizeof(EsFrame);
-  static int resident = 0;  // blocks per SM at this kernel's register and shared-memory use
-  if (!resident) {
+  // resident blocks (blocks per SM at this kernel's register and shared-memory
+  // use, times the SMs) of each device, found on its first launch there
+  constexpr int kDevices = 64;
+  static int resident[kDevices] = {};
+  const int d = (device >= 0 && device < kDevices) ? device : 0;
+  if (!resident[d]) {
     cudaFuncSetAttribute(k_traverse_es<B, K, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int per_sm = 0, dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int per_sm = 0, sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_traverse_es<B, K, 1>, B, smem);
-    resident = std::max(1, per_sm) * std::max(1, sms);
+    resident[d] = std::max(1, per_sm) * std::max(1, sms);
   }
-  const int grid = std::max(1, std::min(resident, (batch + B - 1) / B));
+  const int resident_blocks = resident[d];
+  const int grid = std::max(1, std::min(resident_blocks, (batch + B - 1) / B));
   cudaMemsetAsync(work, 0, sizeof(unsigned), stream);
   k_traverse_es<B, K, 1><<<grid, B, smem, stream>>>(G, tv, deals, sched, batch, rscale, counters, work);
 }

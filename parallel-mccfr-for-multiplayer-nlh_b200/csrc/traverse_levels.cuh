@@ -1,0 +1,449 @@
+// traverse_levels.cuh — level-synchronous external-sampling traversal.
+//
+// The same player-update as k_traverse_es (one depth-first walk per lane), with
+// the work regrouped so that the lanes of a warp do the same kind of work.  A
+// traversal's tree (cfr_gpu.cu:644-860 under external sampling) is cut at the
+// updating player's decision nodes: a *seed* is the root of a traversal or a
+// child of an updating-player node (the state after one of its legal actions),
+// and level L holds the seeds that have L updating-player decisions above them.
+//
+//   expand(L)  one lane per seed of level L: the lane walks the seed's
+//              opponents' nodes (each samples one action and adds its strategy
+//              to the row's strategy sum, as in the depth-first walk), street
+//              changes and terminals, until it reaches a terminal (the seed's
+//              value) or an updating-player node.  That node gets a record (its
+//              state, row slot, legal mask) and every legal action becomes a
+//              seed of level L+1, with the node's regret-matched probability of
+//              that action.  Lanes take seeds from a per-level counter as they
+//              finish, so a warp keeps its lanes busy whatever the walks' lengths.
+//   dfs        seeds that did not fit the buffers (see below) are walked depth
+//              first by the frame-stack walk of k_traverse_es, from the seed.
+//   back(L)    one thread per updating-player node of level L, deepest level
+//              first: it reads its children's values in slot order, adds
+//              fix(v[a]) to the row's per-action accumulators, forms
+//              v_h = sum_a strat[a] * v[a] in the same order as the depth-first
+//              walk, subtracts fix(v_h) (through `su` for the canonical mask) and
+//              hands v_h to its own seed.
+//
+// Every sum that reaches the table is an integer (fixed point) and every draw
+// is keyed by the node's action path, so the rows after an update are
+// bit-identical to the depth-first walk's, whatever the order of the lanes.
+//
+// Buffers.  A level's updating-player nodes and child seeds are appended to
+// two bump-allocated arrays (nodes: 64 B state + 16 B record; seeds: 12 B).  A
+// lane checks, when it picks a seed up, that the arrays still have room for
+// the worst case of every lane that may hold a seed meanwhile (one node and
+// num_actions seeds each); a seed that fails the check is marked and left to
+// the dfs kernel, unwalked.  So no allocation can overflow, and any buffer size
+// gives the same rows.
+#pragma once
+#include "game.cuh"
+#include "table.cuh"
+#include "traverse_ref.cuh"
+#include "traverse_es.cuh"
+
+namespace mccfr {
+
+constexpr int kMaxLevels = 32;
+constexpr uint32_t kSeedDeferred = 0x80000000u;  // walked by the dfs kernel
+constexpr uint32_t kSeedInvalid = 0xFFFFFFFFu;   // child of a node that found no row (table full)
+
+// Per-update counters of the level arrays (zeroed before every update).
+struct LevelCtl {
+  uint32_t seed_count[kMaxLevels];  // seeds of level L (level 0: unused, the batch)
+  uint32_t node_count[kMaxLevels];  // updating-player nodes reached from level L
+  uint32_t grab[kMaxLevels];        // expand work counters
+  uint32_t deferred;                // seeds left to the dfs kernel
+  uint32_t dfs_grab;
+  uint32_t pad[2];
+};
+
+struct LevelBufs {
+  EsState* nodes;     // [node_cap] state at the node (aux = traversal index)
+  uint4* meta;        // [node_cap] {row slot, own seed, first child seed, legal mask (0: none)}
+  uint32_t* child;    // [seed_cap] (node << 3) | action; kSeedDeferred / kSeedInvalid marks
+  float* cstrat;      // [seed_cap] the parent's probability of the seed's action
+  float* value;       // [seed_cap] the seed's value for the updating player
+  LevelCtl* ctl;
+  uint32_t node_cap, seed_cap;
+  int nlev;           // seed levels (the last one is left to the dfs kernel)
+};
+
+// First seed of level L and first node of level L, from the counts of the
+// levels above (final by the time level L runs).
+struct LevelBase {
+  uint32_t seed, seed_next, node, count;
+};
+__device__ __forceinline__ LevelBase level_base(const LevelBufs& lb, int L, int batch) {
+  LevelBase b;
+  uint32_t s = 0, n = 0;
+  for (int l = 0; l < L; ++l) {
+    s += l == 0 ? (uint32_t)batch : lb.ctl->seed_count[l];
+    n += lb.ctl->node_count[l];
+  }
+  b.seed = s;
+  b.count = L == 0 ? (uint32_t)batch : lb.ctl->seed_count[L];
+  b.seed_next = s + b.count;
+  b.node = n;
+  return b;
+}
+
+enum { kLvGoOn = 0, kLvDone = 1, kLvUp = 2 };
+
+// One step of a seed's walk (the descend branch of es_step): the cheap steps
+// (depth cut, fold win, street change, showdown), then at most one decision
+// node.  An opponent's node is done here; at an updating-player node the walk
+// stops with the node's mask, row slot and regrets.
+template <int W>
+__device__ __forceinline__ int lv_step(const GameParams& G, const TableView& tv, uint32_t uid, int up, EsState& cur,
+                                       const DealRec* D, float& value, uint32_t& vm_out, long long& slot_out,
+                                       float* reg, EsCounts& cnt) {
+  const int N = G.N;
+  const uint32_t all_players = (1u << N) - 1;
+  for (int guard = 0; guard < 4; ++guard) {
+    if (cur.depth >= G.max_depth) {
+      value = 0.0f;
+      cnt.terminals++;
+      return kLvDone;
+    }
+    const uint32_t live = all_players & ~(uint32_t)cur.folded;
+    if (__popc(live) == 1) {
+      const int winner = __ffs(live) - 1;
+      const int inv_up = pget(cur.inv, up);
+      value = (winner == up) ? (float)(cur.pot - inv_up) : (float)(-inv_up);
+      cnt.terminals++;
+      return kLvDone;
+    }
+    if (cur.nq != 0) break;
+    if (cur.street < 3) {
+      cur.street++;
+      for (int p = 0; p < kMaxPlayers; ++p) cur.bet[p] = 0;
+      cur.cb = 0;
+      cur.lfr = G.bb;
+      cur.raises = 0;
+      cur.q = 0;
+      cur.nq = 0;
+      for (int i = 1; i <= N; ++i) {
+        const int p = (D->dealer + i) % N;
+        if (!((cur.folded >> p) & 1) && !((cur.allin >> p) & 1)) cur.q |= (uint32_t)p << (4 * cur.nq++);
+      }
+      if (cur.nq > 0) {
+        cur.depth++;
+        continue;
+      }
+    }
+    value = side_pot_payoff(
+        N, up, cur.folded, [&](int q) { return pget(cur.inv, q); }, [&](int q) { return (uint32_t)__ldg(D->rank + q); });
+    cnt.terminals++;
+    return kLvDone;
+  }
+  const int player = (int)(cur.q & 0xF);
+  const int to_call = cur.cb - pget(cur.bet, player);
+  const uint32_t vm = valid_mask(G, cur.pot, es_stack(G, cur, player), to_call, cur.cb, cur.lfr, cur.raises);
+  const uint32_t cw = __ldg(D->ctx + player);
+  uint32_t hb, bkt;
+  if (G.sub_street) {  // exact combo; the river card once it is dealt
+    hb = cw & 0xFFFF;
+    bkt = (cur.street == 3 && G.sub_street == 2) ? (cw >> 16) : 0u;
+  } else {
+    hb = cw & 0xFF;
+    bkt = cur.street ? ((cw >> (8 * cur.street)) & 0xFF) : 0u;
+  }
+  const unsigned long long key = info_key(G, player, hb, bkt, cur.street, cur.abits, cur.path);
+  const long long slot = table_insert<W>(tv, key);
+  load_regrets(tv, slot, reg);
+  cnt.visits++;
+  if (player == up) {
+    vm_out = vm;
+    slot_out = slot;
+    return kLvUp;
+  }
+  // sampled opponent: strategy sum, then one action (es_step's opponent branch)
+  const U4 d = philox(U4{cur.aux, uid, (uint32_t)cur.path, (uint32_t)(cur.path >> 32) | 0x80000000u}, G.seed_lo,
+                      G.seed_hi);
+  const int s = sample_action(G, reg, vm, uniform01(d.x));
+  if (slot >= 0) {
+    if (touch_row(tv, (unsigned long long)slot, uid, vm)) {
+      atomicAdd(row_cnt(tv, slot), (1ull << 32) | 1ull);
+    } else {
+      atomicAdd(row_cnt(tv, slot), 1ull << 32);
+      float strat[kSlots];
+      node_strategy(reg, vm, strat);
+      long long dw[kSlots];
+#pragma unroll
+      for (int a = 0; a < kSlots; ++a) dw[a] = fix_s(strat[a]);
+      add_direct(tv, slot, vm, nullptr, dw);
+    }
+  }
+  es_apply(G, cur, player, s);
+  cur.depth++;
+  return kLvGoOn;
+}
+
+// Start state of a seed: the root (level 0) or the parent node's state after the
+// seed's action.
+__device__ __forceinline__ void lv_seed_state(const GameParams& G, const LevelBufs& lb, const DealRec* deals,
+                                              uint32_t seed, uint32_t w, int batch, int up, EsState& cur,
+                                              const DealRec*& D) {
+  if (seed < (uint32_t)batch) {
+    EsLane tmp;
+    es_begin(G, deals + seed, seed, tmp);
+    cur = tmp.cur;
+    D = deals + seed;
+    return;
+  }
+  const uint32_t node = (w & ~kSeedDeferred) >> 3;
+  const uint4* src = reinterpret_cast<const uint4*>(lb.nodes + node);
+  uint4* dst = reinterpret_cast<uint4*>(&cur);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) dst[i] = __ldcg(src + i);
+  D = deals + cur.aux;
+  es_apply(G, cur, up, (int)(w & 7));
+  cur.depth++;
+}
+
+__device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) { return *(volatile const uint32_t*)p; }
+
+template <int BLOCK, int W>
+__global__ void __launch_bounds__(BLOCK)
+k_level_expand(const GameParams G, const TableView tv, const DealRec* __restrict__ deals,
+               const Sched* __restrict__ sched, int batch, const LevelBufs lb, int L,
+               Counters* __restrict__ counters) {
+  __shared__ LevelBase s_base;
+  if (threadIdx.x == 0) s_base = level_base(lb, L, batch);
+  __syncthreads();
+  const LevelBase B = s_base;
+  if (B.count == 0) return;
+  const int up = sched->player;
+  const uint32_t uid = update_id(sched, G.N);
+  const bool last = L + 1 >= lb.nlev;
+  const int lane = threadIdx.x & 31;
+  // room check at pick-up: every lane of the launch may hold a seed meanwhile
+  const uint32_t holders = min((uint32_t)(gridDim.x * BLOCK), B.count);
+  const unsigned long long need_nodes = (unsigned long long)B.node + holders;
+  const unsigned long long need_seeds = (unsigned long long)B.seed_next + (unsigned long long)holders * G.num_actions;
+  uint32_t* node_count = lb.ctl->node_count + L;
+  uint32_t* next_count = lb.ctl->seed_count + (last ? L : L + 1);
+  EsCounts c{0, 0, 0};
+  unsigned trav = 0, deferred = 0;
+  EsState cur;
+  const DealRec* D = deals;
+  uint32_t seed = 0;
+  bool have = false, more = true;
+  for (;;) {
+    __syncwarp();
+    const bool need = !have && more;
+    const unsigned needm = __ballot_sync(0xFFFFFFFFu, need);
+    if (needm) {
+      const int leader = __ffs(needm) - 1;
+      unsigned base = 0;
+      if (lane == leader) base = atomicAdd(lb.ctl->grab + L, (unsigned)__popc(needm));
+      base = __shfl_sync(0xFFFFFFFFu, base, leader);
+      if (need) {
+        const uint32_t i = base + (uint32_t)__popc(needm & ((1u << lane) - 1u));
+        if (i >= B.count) {
+          more = false;
+        } else {
+          seed = B.seed + i;
+          const uint32_t w = L == 0 ? 0u : __ldcg(lb.child + seed);
+          bool ok = w != kSeedInvalid && !last;
+          if (ok) {
+            ok = need_nodes + ld_volatile(node_count) <= lb.node_cap &&
+                 need_seeds + ld_volatile(next_count) <= lb.seed_cap;
+          }
+          if (w == kSeedInvalid) {
+            // child of a node that found no row: nothing to walk
+          } else if (!ok) {
+            lb.child[seed] = w | kSeedDeferred;
+            deferred++;
+          } else {
+            if (L == 0) lb.child[seed] = 0u;
+            lv_seed_state(G, lb, deals, seed, w, batch, up, cur, D);
+            if (L == 0) trav++;
+            have = true;
+          }
+        }
+      }
+    }
+    if (!__any_sync(0xFFFFFFFFu, have || more)) break;
+    int r = -1;
+    uint32_t vm = 0;
+    long long slot = -1;
+    float reg[kSlots];
+    float v = 0.0f;
+    if (have) {
+      r = lv_step<W>(G, tv, uid, up, cur, D, v, vm, slot, reg, c);
+      if (r == kLvDone) {
+        lb.value[seed] = v;
+        have = false;
+      }
+    }
+    // updating-player nodes of this step: one node record each and one seed per
+    // legal action, allocated for the warp by one lane
+    const bool isup = have && r == kLvUp;
+    const unsigned upm = __ballot_sync(0xFFFFFFFFu, isup);
+    if (upm) {
+      const int k = isup ? __popc(vm) : 0;
+      int incl = k;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+      unsigned jn = 0, jc = 0;
+      if (lane == 0) {
+        jn = atomicAdd(node_count, (unsigned)__popc(upm));
+        jc = atomicAdd(next_count, (unsigned)total);
+      }
+      jn = __shfl_sync(0xFFFFFFFFu, jn, 0);
+      jc = __shfl_sync(0xFFFFFFFFu, jc, 0);
+      if (isup) {
+        const uint32_t j = B.node + jn + (uint32_t)__popc(upm & ((1u << lane) - 1u));
+        const uint32_t cb = B.seed_next + jc + (uint32_t)(incl - k);
+        if (slot < 0) {  // table full (flag raised): the node has no row to update
+          lb.meta[j] = make_uint4(0u, seed, cb, 0u);
+          for (int q = 0; q < k; ++q) lb.child[cb + q] = kSeedInvalid;
+          lb.value[seed] = 0.0f;
+        } else {
+          float strat[kSlots];
+          node_strategy(reg, vm, strat);
+          const uint4* src = reinterpret_cast<const uint4*>(&cur);
+          uint4* dst = reinterpret_cast<uint4*>(lb.nodes + j);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) dst[q] = src[q];
+          lb.meta[j] = make_uint4((uint32_t)slot, seed, cb, vm);
+          uint32_t o = cb;
+#pragma unroll
+          for (int a = 0; a < kSlots; ++a)
+            if ((vm >> a) & 1) {
+              lb.child[o] = (j << 3) | (uint32_t)a;
+              lb.cstrat[o] = strat[a];
+              ++o;
+            }
+        }
+        have = false;
+      }
+    }
+  }
+  if (deferred) atomicAdd(&lb.ctl->deferred, deferred);
+  warp_add_counters(counters, trav, c.visits, 0u, c.terminals, trav * (unsigned)G.N);
+}
+
+// Seeds marked for the depth-first walk, from their start states: persistent
+// lanes scan the seed indices through a work counter (most indices are not
+// marked) and walk each marked seed's subtree with es_step.
+template <int BLOCK, int K, int W>
+__global__ void __launch_bounds__(BLOCK)
+k_level_dfs(const GameParams G, const TableView tv, const DealRec* __restrict__ deals,
+            const Sched* __restrict__ sched, int batch, float rscale, const LevelBufs lb,
+            Counters* __restrict__ counters) {
+  extern __shared__ EsFrame s_frames[];  // [K][BLOCK]
+  if (ld_volatile(&lb.ctl->deferred) == 0) return;
+  __shared__ uint32_t s_total;
+  if (threadIdx.x == 0) {
+    const LevelBase b = level_base(lb, lb.nlev - 1, batch);
+    s_total = b.seed_next;
+  }
+  __syncthreads();
+  const uint32_t total = s_total;
+  const int up = sched->player;
+  const uint32_t uid = update_id(sched, G.N);
+  FrameStack<K> fr;
+  fr.smem = s_frames + threadIdx.x;
+  fr.stride = BLOCK;
+  EsCounts c{0, 0, 0};
+  unsigned trav = 0;
+  const int lane = threadIdx.x & 31;
+  EsLane Ln;
+  uint32_t seed = 0;
+  bool have = false, more = true;
+  for (;;) {
+    __syncwarp();
+    const bool need = !have && more;
+    const unsigned needm = __ballot_sync(0xFFFFFFFFu, need);
+    if (needm) {
+      const int leader = __ffs(needm) - 1;
+      unsigned base = 0;
+      if (lane == leader) base = atomicAdd(&lb.ctl->dfs_grab, (unsigned)__popc(needm));
+      base = __shfl_sync(0xFFFFFFFFu, base, leader);
+      if (need) {
+        const uint32_t i = base + (uint32_t)__popc(needm & ((1u << lane) - 1u));
+        if (i >= total) {
+          more = false;
+        } else {
+          const uint32_t w = __ldcg(lb.child + i);
+          if (w != kSeedInvalid && (w & kSeedDeferred)) {
+            seed = i;
+            const DealRec* D = deals;
+            EsState st;
+            lv_seed_state(G, lb, deals, seed, w, batch, up, st, D);
+            Ln.cur = st;
+            Ln.deal = D;
+            Ln.t = st.aux;
+            Ln.dealer = D->dealer;
+            Ln.sp = 0;
+            Ln.value = 0.0f;
+            Ln.ret = false;
+            if (seed < (uint32_t)batch) trav++;
+            have = true;
+          }
+        }
+      }
+    }
+    if (!__any_sync(0xFFFFFFFFu, have || more)) break;
+    if (have) {
+      const int r = es_step<W>(G, tv, uid, up, rscale, fr, Ln, c);
+      if (r) {
+        lb.value[seed] = r == 1 ? Ln.value : 0.0f;
+        have = false;
+      }
+    }
+  }
+  warp_add_counters(counters, trav, c.visits, c.updates, c.terminals, trav * (unsigned)G.N);
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_level_back(const GameParams G, const TableView tv, const Sched* __restrict__ sched, int batch, float rscale,
+             const LevelBufs lb, int L, Counters* __restrict__ counters) {
+  __shared__ LevelBase s_base;
+  if (threadIdx.x == 0) s_base = level_base(lb, L, batch);
+  __syncthreads();
+  const uint32_t n = lb.ctl->node_count[L];
+  const uint32_t nb = s_base.node;
+  const uint32_t uid = update_id(sched, G.N);
+  unsigned upd = 0;
+  for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < n; i += gridDim.x * BLOCK) {
+    const uint4 m = __ldcg(lb.meta + nb + i);
+    const uint32_t vm = m.w;
+    if (!vm) continue;
+    const unsigned long long slot = m.x;
+    float vh = 0.0f;
+    uint32_t o = m.z;
+#pragma unroll
+    for (int a = 0; a < kSlots; ++a)
+      if ((vm >> a) & 1) {
+        const float v = __ldcg(lb.value + o);
+        const float s = __ldcg(lb.cstrat + o);
+        ++o;
+        atomicAdd(row_da(tv, slot) + a, (unsigned long long)fix_r(v, rscale));
+        vh = __fadd_rn(vh, __fmul_rn(s, v));
+      }
+    const long long fv = fix_r(vh, rscale);
+    atomicAdd(row_cnt(tv, slot), 1ull << 32);
+    if (touch_row(tv, slot, uid, vm)) {
+      atomicAdd(row_su(tv, slot), (unsigned long long)fv);
+    } else {
+      long long dr[kSlots];
+#pragma unroll
+      for (int b = 0; b < kSlots; ++b) dr[b] = -fv;
+      add_direct(tv, slot, vm, dr, nullptr);
+    }
+    upd++;
+    lb.value[m.y] = vh;
+  }
+  warp_add_counters(counters, 0u, 0u, upd, 0u, 0u);
+}
+
+}  // namespace mccfr

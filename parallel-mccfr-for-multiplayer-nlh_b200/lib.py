@@ -33,6 +33,7 @@ KEY_FNV26, KEY_ID64 = 0, 1
 PREFLOP_CHEN64, PREFLOP_CLASS169 = 0, 1
 POSTFLOP_REF_LINEAR, POSTFLOP_RANK_CDF = 0, 1
 PRESET_REF8, PRESET_HU_20BB, PRESET_6MAX_100BB = 0, 1, 2
+FORM_AUTO, FORM_LANES, FORM_LEVELS = 0, 1, 2
 
 
 class Config(Structure):
@@ -44,7 +45,8 @@ class Config(Structure):
         ("raise_cap", c_int32), ("max_depth", c_int32), ("preflop_mode", c_int32),
         ("preflop_buckets", c_int32), ("postflop_mode", c_int32), ("postflop_buckets", c_int32 * 3),
         ("table_log2", c_int32), ("device", c_int32), ("seed", c_uint64),
-        ("key_bits", c_int32), ("reserved", c_int32 * 7),
+        ("key_bits", c_int32), ("traversal_form", c_int32), ("level_log2", c_int32),
+        ("reserved", c_int32 * 5),
     ]
 
     def as_dict(self) -> dict:
@@ -136,6 +138,7 @@ SIGNATURES = {
     "mccfr_get_strategy": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, POINTER(c_size_t)]),
     "mccfr_num_info_sets_active": (c_int, [c_void_p, POINTER(c_longlong)]),
     "mccfr_export_rows": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, POINTER(c_size_t)]),
+    "mccfr_table_digest": (c_int, [c_void_p, c_void_p, c_void_p]),
     "mccfr_export_tables": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),
     "mccfr_import_tables": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),
     "mccfr_save_checkpoint": (c_int, [c_void_p, c_char_p]),

@@ -211,6 +211,13 @@ class GPUCFRTrainer:
         m = n.value
         return {"keys": keys[:m], "regrets": reg[:m], "strategy_sum": ssum[:m], "visits": vis[:m]}
 
+    def digest(self) -> tuple[int, int]:
+        """(checksum, occupied rows) of the table, computed on the device
+        (mccfr_table_digest): equal for tables with the same rows."""
+        d, n = ctypes.c_uint64(), ctypes.c_uint64()
+        L.check(self._lib.mccfr_table_digest(self._h, byref(d), byref(n)), self._h)
+        return int(d.value), int(n.value)
+
     def save_strategy(self, path: str) -> bool:
         return self._lib.mccfr_save_strategy(self._h, str(path).encode()) == L.OK
 

@@ -36,7 +36,11 @@ def test_reference_arm_line():
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
     assert d["config"]["workload"] == "hu-20bb" and d["steps"] == 1 and d["warmup"] == 1
-    assert "visits per traversal" in d["cpu_baseline"]["sample"]
+    assert d["cpu_baseline"]["V_per_traversal"] > 1.0 and "timed iterations" in d["cpu_baseline"]["sample"]
+    # the arm runs the oracle only: the product library is never loaded
+    libs = d["libraries_loaded"]
+    assert any(x.endswith("liboracle.so") for x in libs)
+    assert not any(x.endswith("libmccfr.so") for x in libs)
 
 
 def test_reference_arm_other_ranks_are_silent():
@@ -44,7 +48,7 @@ def test_reference_arm_other_ranks_are_silent():
     assert r.returncode == 0 and r.stdout.strip() == ""
 
 
-def test_apply_roofline_and_sample_text():
+def test_apply_roofline():
     sys.path.insert(0, str(ROOT))
     import bench as b
 
@@ -54,9 +58,29 @@ def test_apply_roofline_and_sample_text():
     assert a["kernel_ms_per_launch"] == 5.0
     assert a["achieved"] == pytest.approx(1_000_000 * 516 / 0.005 / 1e9)
     assert a["frac"] == pytest.approx(a["achieved"] / 6000.0)
-    info = {"seconds": 2.0, "cores": 8, "visits_per_traversal": 1040.0, "visits_per_s": 8.5e6,
-            "raw_traversals_per_s": 8000.0}
-    assert "55.32" in b.cpu_sample_text(16384, info, 55.32)
-    assert "raw traversals/s" in b.cpu_sample_text(16384, info, None)
-    assert b.work_per_traversal("6max-100bb") == pytest.approx(55.32)
-    assert b.work_per_traversal("no-such-workload") is None
+
+
+def test_cpu_baseline_walks_the_handed_over_trees():
+    """cpu_equal_work loads a trainer's rows into the oracle and times that
+    trainer's next update: the oracle's counters there equal the ones of the
+    trainer that produced the rows, run one update further."""
+    sys.path.insert(0, str(ROOT))
+    import bench as b
+    import binding
+    from conftest import mccfr
+
+    L = mccfr.lib
+    cfg = L.preset(L.PRESET_HU_20BB)
+    cfg.table_log2 = 20
+    table = mccfr.hand_table()
+    src = binding.Oracle(cfg, table)
+    src.train(2, 512, threads=2)
+    rows = src.export_rows()
+    c0 = src.counters()
+    src.step(3, 0, 512, threads=2)
+    c1 = src.counters()
+    out = b.cpu_equal_work(rows, cfg, 2, 512, table, 512)
+    assert out["kind"] == "port" and out["value"] > 0 and out["rows_loaded"] == rows["keys"].size
+    assert out["V_per_traversal"] == pytest.approx((c1["visits"] - c0["visits"]) / 512)
+    assert out["U_per_traversal"] == pytest.approx((c1["updates"] - c0["updates"]) / 512)
+    assert "iteration 3, player 0" in out["sample"]

@@ -6,6 +6,7 @@ import ctypes
 from pathlib import Path
 
 import numpy as np
+import pytest
 
 import binding
 from conftest import mccfr
@@ -132,3 +133,43 @@ def test_showdown_masks_match_the_dealt_hands(hand_table):
     split = np.mean([bin(int(x)).count("1") > 1 for x in big])
     assert 0.0 < split < 0.2
     o.close()
+
+
+def test_oracle_presets_and_table_equal_the_product(hand_table):
+    """The oracle's own presets and rank-table generator (used where no device
+    library is loaded) give byte-identical configs and the same table."""
+    L = mccfr.lib
+    for p in (L.PRESET_REF8, L.PRESET_HU_20BB, L.PRESET_6MAX_100BB):
+        assert bytes(binding.config_init(L.Config(), p)) == bytes(L.preset(p))
+    assert np.array_equal(binding.hand_table(), hand_table)
+
+
+def test_row_import_continues_training_and_digest(hand_table):
+    """Rows handed from one oracle to another (import_rows) continue training
+    exactly as the first, and the order-independent digest follows the rows."""
+    L = mccfr.lib
+    cfg = L.preset(L.PRESET_6MAX_100BB)
+    cfg.table_log2, cfg.key_bits = 20, 20
+    a = binding.Oracle(cfg, hand_table)
+    a.train(1, 128, threads=4)
+    b = binding.Oracle(cfg, hand_table)
+    b.import_rows(a.export_rows(), 1)
+    assert a.digest() == b.digest() and a.digest()[1] == a.export_rows()["keys"].size
+    for p in range(6):
+        a.step(2, p, 128, threads=4)
+        b.step(2, p, 128, threads=1)
+    ra, rb = a.export_rows(), b.export_rows()
+    for f in ("keys", "visits", "regrets", "strategy_sum"):
+        assert np.array_equal(np.asarray(ra[f]).view(np.uint8), np.asarray(rb[f]).view(np.uint8)), f
+    assert a.digest() == b.digest()
+    c = binding.Oracle(cfg, hand_table)
+    assert c.digest() == (0, 0)
+    rows = a.export_rows()
+    rows["regrets"][0, 0] = np.nextafter(rows["regrets"][0, 0], np.float32(1e9))
+    c.import_rows(rows, 2)
+    assert c.digest()[0] != a.digest()[0]  # one ulp of one row changes it
+    with pytest.raises(ValueError):
+        bad = dict(rows)
+        bad["keys"] = rows["keys"].copy()
+        bad["keys"][0] = 0
+        c.import_rows(bad, 2)
