@@ -463,13 +463,23 @@ def serving_sweep(m, L, table, rates=(10, 30, 100, 300, 1000), n_requests=48) ->
             r.arrival = float(a)
         srv = sv.ReSolveServer(owner, hbm_budget=32 << 30, traversals=1024)
         res = srv.run(reqs)
-        out[f"lambda_{rate}"] = {**sv.summarize(res), "rounds": srv.rounds, "tables_reused": srv.reused,
-                                 **{k: round(v, 3) for k, v in srv.timing.items()}}
+        line = {**sv.summarize(res), "rounds": srv.rounds, "tables_reused": srv.reused,
+                **{k: round(v, 3) for k, v in srv.timing.items()}}
         srv.close()
+        # the same trace on the plain trainer, one request at a time; equal strategies
+        plain = sv.serve_plain(owner, reqs, traversals=1024)
+        by_rid = {r.rid: r for r in res}
+        same = sum(1 for r in plain if np.array_equal(r.keys, by_rid[r.rid].keys)
+                   and np.array_equal(r.probs.view(np.uint32), by_rid[r.rid].probs.view(np.uint32)))
+        line["plain_trainer"] = {**sv.summarize(plain), "strategies_bit_identical": f"{same}/{len(plain)}"}
+        out[f"lambda_{rate}"] = line
     owner.close()
     out["workload"] = (f"{n_requests} requests per rate: turn/river board, 2-6 players, pot U[2,200]BB, "
-                       "Dirichlet(0.5) ranges, 3-5 sizes + all-in, budget log-uniform [2e3,5e4] traversals per "
-                       "player, 1024 traversals per update, 100BB stacks, seed 4")
+                       "Dirichlet(0.5) ranges, 3-6 sizes drawn (at most 5 kept: fold, check/call, the sizes and "
+                       "all-in fill the 8 action slots of a row) + all-in, 100BB stacks, seed 4. Budget unit: "
+                       "iterations of the one-traversal-per-player form, log-uniform [2e3,5e4] = traversals per "
+                       "player, spent 1024 per player-update. plain_trainer: the same trace served one request "
+                       "at a time by train() in arrival order")
     return out
 
 
@@ -522,46 +532,64 @@ SEVEN_CARD_CATEGORIES = [23294460, 58627800, 31433400, 6461620, 6180020, 4047644
 CATEGORY_START = [1, 1278, 4138, 4996, 5854, 5864, 7141, 7297, 7453, 7463]
 
 
-def c4_showdown(m, L, table, total=1 << 28, chunk=1 << 24) -> dict:
-    """Showdown microbench: `total` uniform 7-card hands (seeded, without
-    replacement within a hand) evaluated on the device by mccfr_eval7_device,
-    timed with its CUDA events; 7 dependent rank-table gathers (28 B) per hand.
-    The category frequencies are checked against the exact counts."""
+def c4_showdown(m, L, table, total=1 << 28, chunk=1 << 24, deals6=1 << 24) -> dict:
+    """Showdown microbench, both parts seeded by Philox seed 3 on the device.
+    7-card: `total` uniform 7-card hands (mccfr_deal_eval7: drawn and ranked in
+    one kernel, 7 dependent gathers = 28 B of rank-table reads per hand); the
+    category frequencies are checked against the exact counts.  6-seat:
+    `deals6` deals of training's 6-player deal (update 1, player 0) with the
+    board walked once for all seats (mccfr_showdown_masks: 5 + 2 x 6 gathers =
+    68 B per deal) and 6-bit winner masks; seat symmetry and the split rate are
+    checked.  Kernel time from the library's CUDA events."""
     import ctypes
 
     import numpy as np
     import torch
 
-    t = m.GPUCFRTrainer(config=L.preset(L.PRESET_HU_20BB), table_log2=10)
-    t.set_hand_table(table)
     lib = L.load()
-    gen = torch.Generator(device="cuda")
-    gen.manual_seed(3)
+    peak, kind = measured_peak()
+    cfg = L.preset(L.PRESET_6MAX_100BB)
+    cfg.seed, cfg.table_log2 = 3, 10
+    t = m.GPUCFRTrainer(config=cfg)
+    t.set_hand_table(table)
     ranks = torch.empty(chunk, dtype=torch.int16, device="cuda")
     hist = torch.zeros(7463, dtype=torch.int64, device="cuda")
     ms_total = 0.0
-    for _ in range(total // chunk):
-        cards = torch.rand(chunk, 52, device="cuda", generator=gen).argsort(dim=1)[:, :7].to(torch.uint8).contiguous()
-        torch.cuda.synchronize()  # the library evaluates on its own stream
+    torch.cuda.synchronize()
+    for stream in range(total // chunk):
         ms = ctypes.c_float()
-        L.check(lib.mccfr_eval7_device(t.handle, ctypes.c_void_p(cards.data_ptr()), ctypes.c_void_p(ranks.data_ptr()),
-                                       chunk, ctypes.byref(ms)))
+        L.check(lib.mccfr_deal_eval7(t.handle, stream, chunk, ctypes.c_void_p(ranks.data_ptr()), ctypes.byref(ms)))
         ms_total += ms.value
         hist += torch.bincount(ranks.to(torch.int64) & 0xFFFF, minlength=7463)[:7463]
-        del cards
-    t.close()
     h = hist.cpu().numpy()
     n = (total // chunk) * chunk
     obs = np.array([h[CATEGORY_START[i]:CATEGORY_START[i + 1]].sum() for i in range(9)], dtype=np.float64)
     p = np.array(SEVEN_CARD_CATEGORIES, dtype=np.float64) / 133784560.0
     z = (obs / n - p) / np.sqrt(p * (1 - p) / n)
     evals = n / (ms_total / 1e3)
-    peak, kind = measured_peak()
+    # 6-seat shared-board showdown of training's deals
+    masks = torch.empty(deals6, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    ms6 = ctypes.c_float()
+    L.check(lib.mccfr_showdown_masks(t.handle, 1, 0, deals6, ctypes.c_void_p(masks.data_ptr()), ctypes.byref(ms6)))
+    mk = masks.to(torch.int64)
+    wins = [int(((mk >> q) & 1).sum().item()) for q in range(6)]
+    pop = sum(((mk >> q) & 1) for q in range(6))
+    split = float((pop > 1).double().mean().item())
+    bad = int(((mk == 0) | (mk >= 64)).sum().item())
+    t.close()
+    deals_s = deals6 / (ms6.value / 1e3)
     return {"hands": n, "hand_evals_per_s": evals, "kernel_ms": ms_total,
             "gather_gbs": 28.0 * evals / 1e9, "gather_frac_of_hbm_peak": 28.0 * evals / 1e9 / peak,
             "category_max_abs_z": float(np.abs(z).max()), "invalid_ranks": int(h[0]),
-            "workload": "2^28 uniform 7-card hands in chunks of 2^24 (torch generator seed 3, cards on the "
-                        "device), k_eval7: one thread per hand, 7 dependent gathers into the 130 MB rank table"}
+            "six_seat": {"deals": deals6, "kernel_ms": ms6.value, "deals_per_s": deals_s,
+                         "hand_evals_per_s": 6 * deals_s, "gather_gbs": 68.0 * deals_s / 1e9,
+                         "seat_wins": wins, "split_rate": split, "invalid_masks": bad},
+            "workload": "Philox seed 3 on the device. 7-card: 2^28 hands in 16 calls of 2^24 (stream = call "
+                        "index), k_deal_eval7 draws and ranks each hand (7 dependent gathers into the 130 MB rank "
+                        "table). 6-seat: 2^24 deals of training's 6-player deal (iteration 1, player 0), "
+                        "k_showdown_masks (board walked once, 2 gathers per seat, winner/split mask per deal); "
+                        "both bit-exact with the oracle in tests/test_gpu_showdown.py"}
 
 
 def hu_full_exploitability(m, L, table, iters: int, stride: int) -> dict:

@@ -286,6 +286,24 @@ int mccfr_eval7(mccfr_handle* h, const uint8_t* cards, uint16_t* ranks, size_t n
 int mccfr_eval7_device(mccfr_handle* h, const uint8_t* dev_cards,
                        uint16_t* dev_ranks, size_t n, float* ms);
 
+/* ---- showdown microbenchmark ---------------------------------------------
+   No reference counterpart as entry points; they time the gathers of the
+   reference's rank chains and showdown (cfr_gpu.cu:114-150, 694-753) alone.
+   mccfr_deal_eval7: hands i = 0..n-1, each 7 distinct cards drawn on the device
+   by partial Fisher-Yates over the 52 cards, j = k + (w_k * (52 - k)) >> 32, with
+   the words w_0..w_6 of Philox4x32-10 (key = the handle's seed) at counters
+   (i mod 2^32, stream, 0x300, i >> 32) and (..., 0x301, ...); dev_ranks[i] is the
+   hand's rank (1..7462).
+   mccfr_showdown_masks: the deals of traversals 0..n-1 of update (iteration,
+   player), the cards training deals; each seat's 7-card rank with the 5-card
+   board walked once for all seats (5 + 2 per seat gathers); dev_masks[t] has bit
+   q set when seat q holds the best rank (several bits: a split).  Full game only.
+   Both run on the handle's stream and return after the kernel; *ms (optional)
+   receives its CUDA-event time. */
+int mccfr_deal_eval7(mccfr_handle* h, uint32_t stream, size_t n, uint16_t* dev_ranks, float* ms);
+int mccfr_showdown_masks(mccfr_handle* h, long long iteration, int player, size_t n,
+                         uint8_t* dev_masks, float* ms);
+
 /* ---- batched form: many tables in one persistent kernel ------------------
    No reference counterpart.  A batch groups existing handles
    (tables), each with its own game, table and schedule; one iteration runs
@@ -375,11 +393,14 @@ int mccfr_get_progress(mccfr_handle* h, long long* next_iteration, int* next_pla
    as mccfr_eval7, with its staging in a static device array of
    MCCFR_EVAL7_STATIC_MAX_HANDS hands (about 2.25 MiB, held by every GPU that
    loads the library until exit).  dev_table is the caller's device copy of the
-   32,487,834-entry rank table; cards (7 per hand, 0..51) and ranks are host
-   buffers; runs on the current device.  n above the maximum returns
+   32,487,834-entry rank table and must be device (or managed) memory: a host
+   pointer returns MCCFR_ERR_INVALID_ARG; cards (7 per hand, 0..51) and ranks
+   are host buffers; runs on the current device.  n above the maximum returns
    MCCFR_ERR_INVALID_ARG.  The first call on a device looks up the array's
-   address and must come before any stream capture.  Calls share the array, so
-   calls that overlap on the GPU race: serialise them. */
+   address and must come before any stream capture; the address holds for the
+   life of the device's context (do not call again on a device after
+   cudaDeviceReset).  Calls share the array, so calls that overlap on the GPU
+   race: serialise them. */
 #define MCCFR_EVAL7_STATIC_MAX_HANDS (1u << 18)
 int mccfr_eval7_static(const int32_t* dev_table, const uint8_t* cards, uint16_t* ranks, size_t n);
 

@@ -43,6 +43,7 @@ def lib() -> ctypes.CDLL:
         o.orc_export_rows.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, POINTER(c_size_t)]
         o.orc_table_digest.argtypes = [c_void_p, c_void_p, c_void_p]
         o.orc_config_init.argtypes = [c_void_p, c_int]
+        o.orc_deal_eval7.argtypes = [c_void_p, ctypes.c_uint64, c_uint32, c_size_t, c_void_p]
         o.orc_hand_table_generate.argtypes = [c_void_p, c_size_t]
         o.orc_import_rows.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_longlong]
         o.orc_get_strategy.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, POINTER(c_size_t)]
@@ -207,6 +208,13 @@ def eval7(table: np.ndarray, cards: np.ndarray) -> np.ndarray:
     c = np.ascontiguousarray(cards, dtype=np.uint8).reshape(-1, 7)
     out = np.empty(c.shape[0], dtype=np.uint16)
     lib().orc_eval7(_p(table), _p(c), _p(out), c.shape[0])
+    return out
+
+
+def deal_eval7(table: np.ndarray, seed: int, stream: int, n: int) -> np.ndarray:
+    """Ranks of the showdown microbenchmark's hands 0..n-1 (orc_deal_eval7)."""
+    out = np.empty(n, dtype=np.uint16)
+    assert lib().orc_deal_eval7(_p(table), int(seed), int(stream), n, _p(out)) == 0
     return out
 
 

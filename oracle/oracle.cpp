@@ -1452,6 +1452,30 @@ int orc_showdown_masks(void* h, long long iteration, int player, int n, uint8_t*
   return 0;
 }
 
+// Hands i = 0..n-1 of the showdown microbenchmark: 7 distinct cards by partial
+// Fisher-Yates (the deal's multiply-shift, cfr_gpu.cu:460-470) from Philox words
+// keyed by the seed at counters (i lo, stream, 0x300 | 0x301, i hi), ranked in the
+// reference's order (hand_eval.cpp:134-143).
+int orc_deal_eval7(const int32_t* T, uint64_t seed, uint32_t stream, size_t n, uint16_t* ranks) {
+  if (!T || (n && !ranks)) return MCCFR_ERR_INVALID_ARG;
+  for (size_t i = 0; i < n; ++i) {
+    const uint32_t lo = (uint32_t)i, hi = (uint32_t)((uint64_t)i >> 32);
+    const U4 a = philox(U4{lo, stream, 0x300u, hi}, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const U4 b = philox(U4{lo, stream, 0x301u, hi}, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const uint32_t w[7] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z};
+    uint8_t deck[52];
+    for (int c = 0; c < 52; ++c) deck[c] = (uint8_t)c;
+    int cards[7];
+    for (int k = 0; k < 7; ++k) {
+      const int j = k + (int)(((uint64_t)w[k] * (uint64_t)(52 - k)) >> 32);
+      std::swap(deck[k], deck[j]);
+      cards[k] = deck[k];
+    }
+    ranks[i] = decode16((uint16_t)(chain(T, cards, 7) & 0xFFFF));
+  }
+  return 0;
+}
+
 // Nodes per tree depth in the last level-synchronous update, summed over its
 // traversals; returns the number of depths (at most `cap` are written).
 int orc_wave_hist(void* h, int64_t* out, int cap) {

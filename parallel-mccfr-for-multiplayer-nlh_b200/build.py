@@ -20,7 +20,7 @@ LIB = PKG / "libmccfr.so"
 ORACLE_DIR = ROOT / "oracle"
 
 SOURCES = ["mccfr.cu", "eval_static.cu", "best_response.cu", "handtable.cpp", "abstraction.cpp"]
-HEADERS = ["game.cuh", "table.cuh", "traverse_ref.cuh", "traverse_es.cuh", "traverse_levels.cuh", "batched.cuh",
+HEADERS = ["game.cuh", "table.cuh", "traverse_ref.cuh", "traverse_es.cuh", "traverse_levels.cuh", "showdown.cuh", "batched.cuh",
            "handtable.h", "best_response.h"]
 
 NVCC_FLAGS = [

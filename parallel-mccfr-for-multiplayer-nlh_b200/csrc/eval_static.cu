@@ -16,7 +16,11 @@
 // array and the array keeps the last call's contents; calls that overlap on the
 // GPU (from several host threads) race on it, so callers must serialise them.
 // Nothing in the array needs to start at zero: each call writes every card and
-// rank slot it reads back.
+// rank slot it reads back.  The looked-up address lives as long as the device's
+// context: after cudaDeviceReset the array may sit elsewhere, so a process that
+// resets a device must not call this entry point on that device again.
+// dev_table must be device memory (or managed memory): a host pointer is
+// refused with MCCFR_ERR_INVALID_ARG instead of reaching the kernel.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -80,6 +84,12 @@ extern "C" int mccfr_eval7_static(const int32_t* dev_table, const uint8_t* cards
   if (n == 0) return MCCFR_OK;
   for (size_t i = 0; i < 7 * n; ++i)
     if (cards[i] > 51) return MCCFR_ERR_INVALID_ARG;
+  cudaPointerAttributes attr;
+  if (cudaPointerGetAttributes(&attr, dev_table) != cudaSuccess) {
+    cudaGetLastError();
+    return MCCFR_ERR_INVALID_ARG;
+  }
+  if (attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged) return MCCFR_ERR_INVALID_ARG;
   uint8_t* base = nullptr;
   const int rc = scratch_address(&base);
   if (rc) return rc;

@@ -32,6 +32,7 @@
 #include "traverse_ref.cuh"
 #include "traverse_es.cuh"
 #include "traverse_levels.cuh"
+#include "showdown.cuh"
 #include "batched.cuh"
 #include "best_response.h"
 
@@ -1434,8 +1435,12 @@ int mccfr_import_tables(mccfr_handle* h, const float* regrets, const float* stra
   if (!rc) {
     e = cudaMemcpyAsync(dr, regrets, need * 4, cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(ds, strategy_sum, need * 4, cudaMemcpyHostToDevice, h->stream);
+    // The dense tables replace the table's contents, as the reference's load
+    // overwrites both arrays (cfr_gpu.cu:1526-1527): rows are cleared first, then
+    // every slot with a non-zero value becomes a row (an all-zero slot reads as
+    // zeros either way).
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->d_block, 0, h->block_bytes, h->stream);
     if (e == cudaSuccess) {
-      // Rows keep their keys; values are replaced (zeros where the dense table is zero).
       k_import_dense<<<148 * 16, 256, 0, h->stream>>>(h->tv, dr, ds, MCCFR_REF_TABLE_SIZE);
       e = cudaStreamSynchronize(h->stream);
     }
@@ -1443,7 +1448,10 @@ int mccfr_import_tables(mccfr_handle* h, const float* regrets, const float* stra
   }
   cudaFree(dr);
   cudaFree(ds);
-  if (!rc) rc = check_device_error(h);
+  if (!rc) {
+    h->touched_last = 0;
+    rc = check_device_error(h);
+  }
   return rc;
 }
 
@@ -1656,6 +1664,41 @@ int mccfr_eval7(mccfr_handle* h, const uint8_t* cards, uint16_t* ranks, size_t n
   cudaFree(dc);
   cudaFree(dr);
   return rc;
+}
+
+int mccfr_deal_eval7(mccfr_handle* h, uint32_t stream, size_t n, uint16_t* dev_ranks, float* ms) {
+  if (!h || (n && !dev_ranks)) return MCCFR_ERR_INVALID_ARG;
+  if (!h->has_table) return fail(h, MCCFR_ERR_NO_HAND_TABLE, "load a hand-rank table first");
+  CK(cudaSetDevice(h->device));
+  CK(cudaEventRecord(h->ev[0], h->stream));
+  if (n)
+    k_deal_eval7<256><<<grid_for((long long)n, 256), 256, 0, h->stream>>>(h->d_hr, h->gp.seed_lo, h->gp.seed_hi,
+                                                                         stream, n, dev_ranks);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(h->ev[1], h->stream));
+  CK(cudaEventSynchronize(h->ev[1]));
+  if (ms) cudaEventElapsedTime(ms, h->ev[0], h->ev[1]);
+  return MCCFR_OK;
+}
+
+int mccfr_showdown_masks(mccfr_handle* h, long long iteration, int player, size_t n, uint8_t* dev_masks,
+                         float* ms) {
+  if (!h || iteration < 1 || player < 0 || player >= h->cfg.num_players || (n && !dev_masks) ||
+      n > 0xFFFFFFFFull)
+    return MCCFR_ERR_INVALID_ARG;
+  if (h->gp.sub_street) return fail(h, MCCFR_ERR_INVALID_ARG, "showdown masks are defined for the full game");
+  if (!h->has_table) return fail(h, MCCFR_ERR_NO_HAND_TABLE, "load a hand-rank table first");
+  CK(cudaSetDevice(h->device));
+  const uint32_t uid = (uint32_t)((iteration - 1) * h->cfg.num_players + player);
+  CK(cudaEventRecord(h->ev[0], h->stream));
+  if (n)
+    k_showdown_masks<256><<<grid_for((long long)n, 256), 256, 0, h->stream>>>(h->gp, h->d_hr, uid, (unsigned)n,
+                                                                             dev_masks);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(h->ev[1], h->stream));
+  CK(cudaEventSynchronize(h->ev[1]));
+  if (ms) cudaEventElapsedTime(ms, h->ev[0], h->ev[1]);
+  return MCCFR_OK;
 }
 
 }  // extern "C"

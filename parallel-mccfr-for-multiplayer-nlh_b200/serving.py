@@ -124,6 +124,7 @@ class Result:
     keys: np.ndarray = field(repr=False)
     probs: np.ndarray = field(repr=False)
     cancelled: bool = False     # withdrawn by cancel(): no strategy
+    error: str = ""             # refused: the request can never be admitted (no strategy)
 
     @property
     def latency_ms(self) -> float:
@@ -144,7 +145,10 @@ class ReSolveServer:
 
     cancel(rid), from any thread, withdraws a request: one not yet admitted is
     dropped, one being solved retires after the current round without exporting
-    its strategy, and its table goes back to the pool.  round_fn and create_fn
+    its strategy, and its table goes back to the pool.  A request that does not
+    fit an idle server (its table above the budget, or above the free device
+    memory with every pooled table freed) is refused with an error result
+    instead of blocking the queue.  round_fn and create_fn
     replace the device round (batch_round) and the table creation, so the loop's
     host logic can run against stand-ins."""
 
@@ -163,6 +167,7 @@ class ReSolveServer:
         self.pool: dict[int, list[GPUCFRTrainer]] = {}
         self.reused = 0
         self.cancelled = 0
+        self.refused = 0
         self._round = round_fn or batch_round
         self._create = create_fn or self._create_subgame
         self._lock = threading.Lock()
@@ -214,8 +219,7 @@ class ReSolveServer:
             self.reused += 1
         else:
             t = self._create(cfg, req)
-        per_player = max(1, math.ceil(req.budget / self.traversals))
-        return Solve(req, t, per_player * req.players, admitted=now)
+        return Solve(req, t, updates_for(req, self.traversals) * req.players, admitted=now)
 
     def close(self) -> None:
         """Frees the pooled tables."""
@@ -252,6 +256,16 @@ class ReSolveServer:
                 active.append(self._start(req, time.perf_counter() - t0))
                 held += table_bytes(req)
             self.timing["admit_s"] += time.perf_counter() - ta
+            if not active and queue:
+                # nothing runs and no pooled table is left to free, yet the head of
+                # the queue does not fit: it never will, so it is refused rather
+                # than left to block the requests behind it
+                req = queue.pop(0)
+                self.refused += 1
+                results.append(Result(req.rid, req.arrival, now, time.perf_counter() - t0, *none,
+                                      error=f"needs {table_bytes(req)} device bytes; budget {self.hbm_budget}, "
+                                            f"free {self.free_memory()}"))
+                continue
             if not active:
                 if pending:
                     time.sleep(max(0.0, min(0.001, pending[0].arrival - now)))
@@ -280,15 +294,57 @@ class ReSolveServer:
         return results
 
 
+def updates_for(req: Request, traversals: int) -> int:
+    """Player-updates a request's budget buys: the budget counts traversals per
+    player (iterations of the one-traversal-per-player form), spent
+    `traversals` at a time."""
+    return max(1, math.ceil(req.budget / traversals))
+
+
+def serve_plain(owner: GPUCFRTrainer, requests: list[Request], traversals: int = 256,
+                realtime: bool = True) -> list[Result]:
+    """The same requests on the plain trainer, one request at a time in arrival
+    order: each is trained alone by `train` (one CUDA graph per iteration, every
+    player-update of `traversals` traversals) until its budget is spent, then its
+    strategy is copied out.  Tables are reused by capacity like the server's.
+    The comparison point for continuous batching: same updates, same results."""
+    pending = sorted(requests, key=lambda r: r.arrival)
+    pool: dict[int, GPUCFRTrainer] = {}
+    results: list[Result] = []
+    t0 = time.perf_counter()
+    try:
+        for req in pending:
+            now = time.perf_counter() - t0
+            if realtime and req.arrival > now:
+                time.sleep(req.arrival - now)
+            admitted = time.perf_counter() - t0
+            cfg = request_config(req)
+            t = pool.get(req.table_log2)
+            if t is None:
+                t = GPUCFRTrainer.subgame(cfg, req.street, req.pot, req.board, req.ranges)
+                t.share_hand_table(owner)
+                pool[req.table_log2] = t
+            else:
+                t.reset_subgame(cfg, req.street, req.pot, req.board, req.ranges)
+            t.train(updates_for(req, traversals), traversals, verbose=False)
+            keys, probs = t.strategy_arrays()
+            results.append(Result(req.rid, req.arrival, admitted, time.perf_counter() - t0, keys, probs))
+    finally:
+        for t in pool.values():
+            t.close()
+    return results
+
+
 def poisson_arrivals(rng: np.random.Generator, n: int, rate: float) -> np.ndarray:
     return np.cumsum(rng.exponential(1.0 / rate, size=n))
 
 
 def summarize(results: list[Result]) -> dict:
-    """Latency percentiles and throughput of the solved requests; cancelled ones
-    are counted apart."""
-    done = [r for r in results if not r.cancelled]
-    out = {"requests": len(done), "cancelled": len(results) - len(done)}
+    """Latency percentiles and throughput of the solved requests; cancelled and
+    refused ones are counted apart."""
+    done = [r for r in results if not r.cancelled and not r.error]
+    out = {"requests": len(done), "cancelled": sum(1 for r in results if r.cancelled),
+           "refused": sum(1 for r in results if r.error)}
     if not done:
         return out
     lat = np.array([r.latency_ms for r in done])

@@ -107,3 +107,28 @@ def test_refuses_other_games_and_bad_files(hand_table, tmp_path):
     rows_equal(d.export_rows(), a.export_rows())
     for t in (a, c, d):
         t.close()
+
+
+def test_reference_checkpoint_replaces_a_trained_table(hand_table, tmp_path):
+    """Loading the reference-layout checkpoint into a handle that has trained
+    on its own replaces every row, as the reference's load overwrites both
+    arrays (cfr_gpu.cu:1526-1527): afterwards the handle holds exactly the
+    saved rows, none of its own."""
+    cfg = L.preset(L.PRESET_REF8)
+    cfg.table_log2 = 26
+    a = trainer(cfg, hand_table)
+    a.train(2, 4096, verbose=False)
+    ck = tmp_path / "a.ckpt"
+    assert a.save_checkpoint(str(ck))
+    b_cfg = L.Config.from_buffer_copy(cfg)
+    b_cfg.seed = 7  # other deals: rows that A never touched
+    b = trainer(b_cfg, hand_table)
+    b.train(3, 4096, verbose=False)
+    assert b.load_checkpoint(str(ck))
+    ra, rb = a.export_rows(), b.export_rows()
+    live = (np.abs(ra["regrets"]).sum(1) + np.abs(ra["strategy_sum"]).sum(1)) > 0
+    assert np.array_equal(ra["keys"][live], rb["keys"])
+    assert np.array_equal(ra["regrets"][live].view(np.uint32), rb["regrets"].view(np.uint32))
+    assert np.array_equal(ra["strategy_sum"][live].view(np.uint32), rb["strategy_sum"].view(np.uint32))
+    a.close()
+    b.close()

@@ -184,4 +184,46 @@ def test_summary_leaves_out_cancelled_requests():
     s = sv.summarize(res)
     assert s["requests"] == 2 and s["cancelled"] == 1
     assert s["p50_ms"] == pytest.approx(200.0) and s["mean_ms"] == pytest.approx(200.0)
-    assert sv.summarize(res[2:]) == {"requests": 0, "cancelled": 1}
+    assert sv.summarize(res[2:]) == {"requests": 0, "cancelled": 1, "refused": 0}
+
+
+def test_request_that_can_never_fit_is_refused_not_spun_on():
+    """A request whose table exceeds the whole budget, at the head of the queue
+    of an idle server, is refused with an error result (the loop used to retry
+    it forever); the requests behind it are served."""
+    reqs = _same_size_requests(3)
+    big = reqs[0]
+    big.table_log2 = 21
+    need_small = sv.table_bytes(reqs[1])
+    assert sv.table_bytes(big) > 4 * need_small
+
+    def round_fn(trainers, traversals, tuning):
+        for t in trainers:
+            t.rounds += 1
+
+    srv = sv.ReSolveServer(None, hbm_budget=4 * need_small, max_active=2, free_memory=lambda: 100 << 30,
+                           traversals=256, round_fn=round_fn, create_fn=lambda cfg, req: _FakeSolver())
+    res = {r.rid: r for r in srv.run(reqs, realtime=False)}
+    assert res[big.rid].error and "device bytes" in res[big.rid].error and res[big.rid].keys.size == 0
+    for r in reqs[1:]:
+        assert not res[r.rid].error and res[r.rid].keys.tolist() == [7]
+    assert srv.refused == 1
+    s = sv.summarize(list(res.values()))
+    assert s["requests"] == 2 and s["refused"] == 1
+
+
+def test_device_memory_short_of_a_request_refuses_it():
+    """Free device memory below a request's table (plus the 1 GiB reserve) with
+    nothing running: refused the same way."""
+    reqs = _same_size_requests(1)
+    srv = sv.ReSolveServer(None, hbm_budget=1 << 40, free_memory=lambda: 1 << 20, traversals=256,
+                           round_fn=lambda *a: None, create_fn=lambda cfg, req: _FakeSolver())
+    res = srv.run(reqs, realtime=False)
+    assert len(res) == 1 and res[0].error
+
+
+def test_budget_counts_traversals_per_player():
+    reqs = _same_size_requests(1)
+    assert sv.updates_for(reqs[0], 256) == 4
+    reqs[0].budget = 1000
+    assert sv.updates_for(reqs[0], 256) == 4  # rounded up

@@ -42,4 +42,9 @@ def test_static_entry_point_matches_allocating_one(hand_table):
     cards = np.zeros((n, 7), dtype=np.uint8)
     out = np.zeros(n, dtype=np.uint16)
     assert lib.mccfr_eval7_static(L.c_void_p(dev_table.data_ptr()), L.ptr(cards), L.ptr(out), n) == 1
+    # a host copy of the table is refused before any kernel could read it
+    cards = np.zeros((4, 7), dtype=np.uint8)
+    cards[:] = np.arange(7)
+    out = np.zeros(4, dtype=np.uint16)
+    assert lib.mccfr_eval7_static(L.ptr(hand_table), L.ptr(cards), L.ptr(out), 4) == 1
     tr.close()
