@@ -74,13 +74,20 @@ def make_config(L, workload: str, rank: int = 0):
 
 
 def apply_roofline(s0, s1, launches: int, peak: float) -> dict:
-    """The apply kernel's share of a step against the HBM roofline: 516 B per touched
-    row (the 256-byte record read and written, the list entry read)."""
+    """The apply kernel's share of a step against the HBM roofline: per touched
+    row its first 128-byte line read and written and its 4-byte list entry read
+    (260 B), plus the second line read and written (256 B) for the rows that
+    hold the updating player's accumulators; rows counted on the device for the
+    last player-update."""
     ms = (s1.apply_ms - s0.apply_ms) / max(1, launches)
     rows = int(s1.touched_last)
-    gbs = rows * 516.0 / (ms / 1e3) / 1e9 if ms > 0 else None
+    wide = int(getattr(s1, "wide_rows_last", 0))
+    nbytes = rows * 260.0 + wide * 256.0
+    gbs = nbytes / (ms / 1e3) / 1e9 if ms > 0 else None
     return {"kernel": "k_apply", "kernel_ms_per_launch": ms, "touched_rows_last_update": rows,
-            "bytes_per_row": 516, "achieved": gbs, "unit": "GB/s", "frac": gbs / peak if gbs else None}
+            "wide_rows_last_update": wide, "bytes_per_launch": nbytes,
+            "bytes_per_row": "260 (first line + list entry) + 256 for rows with regret accumulators",
+            "achieved": gbs, "unit": "GB/s", "frac": gbs / peak if gbs else None}
 
 
 def over_ranks(ms: float, traversals: int, e2e_s: float, device) -> tuple[float, float, float]:

@@ -119,7 +119,7 @@ typedef struct mccfr_config {
      not part of the game (a v2 checkpoint loads into any form). */
   int32_t traversal_form;
   /* MCCFR_FORM_LEVELS only: capacity of the updating-player node buffer as
-     log2 of the node records (80 B each; the child buffer holds four times as
+     log2 of the node records (80 B each; the child buffer holds eight times as
      many 12 B entries); 0 = sized from the batch.  Subtrees that do not fit are
      walked depth first inside the same update, with the same result. */
   int32_t level_log2;
@@ -157,7 +157,10 @@ typedef struct mccfr_stats {
   double last_traverse_ms;
   double last_apply_ms;
   int32_t device_error;      /* sticky kernel error bits */
-  int32_t reserved[7];
+  /* rows of the last player-update whose second 128-byte line (the updating
+     player's regret accumulators) was folded as well as the first */
+  int32_t wide_rows_last;
+  int32_t reserved[6];
 } mccfr_stats;
 
 /* One traversal's record from mccfr_step_trace (reference sampling mode). */

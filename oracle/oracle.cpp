@@ -1592,12 +1592,24 @@ int orc_import_rows(void* h, const uint64_t* keys, const float* R, const float* 
   for (size_t i = 0; i < n; ++i)
     if (keys[i] == 0) return MCCFR_ERR_INVALID_ARG;
   O.rows = RowTable();
-  for (size_t i = 0; i < n; ++i) {
-    Row& r = O.rows[keys[i]];
-    std::memcpy(r.r, R + 8 * i, 32);
-    std::memcpy(r.s, S + 8 * i, 32);
-    r.visits = visits[i];
-  }
+  // rows grouped by shard, then each shard filled by one host thread
+  std::vector<std::vector<uint32_t>> by_shard(kRowShards);
+  for (size_t i = 0; i < n; ++i) by_shard[row_shard(keys[i])].push_back((uint32_t)i);
+  std::atomic<int> next{0};
+  auto fill = [&]() {
+    for (int sh; (sh = next.fetch_add(1)) < kRowShards;)
+      for (uint32_t i : by_shard[sh]) {
+        Row& r = O.rows.shard[sh][keys[i]];
+        std::memcpy(r.r, R + 8 * (size_t)i, 32);
+        std::memcpy(r.s, S + 8 * (size_t)i, 32);
+        r.visits = visits[i];
+      }
+  };
+  const int nt = std::max(1, std::min(kRowShards, (int)std::thread::hardware_concurrency()));
+  std::vector<std::thread> th;
+  for (int t = 1; t < nt; ++t) th.emplace_back(fill);
+  fill();
+  for (auto& x : th) x.join();
   O.iterations_done = iterations_done;
   return 0;
 }

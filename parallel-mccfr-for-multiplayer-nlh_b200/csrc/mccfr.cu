@@ -64,6 +64,7 @@ __device__ __forceinline__ void apply_rows(const GameParams& G, const TableView&
   const double s32 = 2.3283064365386962890625e-10;  // 2^-32
   const int a = threadIdx.x & 7;
   const unsigned gmask = 0xFFu << (threadIdx.x & 24);
+  unsigned wide = 0;  // rows whose second line was folded too (counted by lane 0 of each group)
   for (unsigned i = group; i < n; i += ngroups) {
     const unsigned long long slot = tv.touched[i];
     const uint32_t m = (uint32_t)(*row_tag(tv, slot) & 0xFF);
@@ -77,8 +78,9 @@ __device__ __forceinline__ void apply_rows(const GameParams& G, const TableView&
     long long* dsp = reinterpret_cast<long long*>(row_ds(tv, slot));
     const float r_a = regp[a];
     const float s_a = ssp[a];
-    const long long da_a = dap[a];
-    const long long ds_a = (flags & 1u) ? dsp[a] : 0ll;
+    // a row visited only by sampled opponents has nothing on its second line
+    const long long da_a = (flags & kFlagDa) ? dap[a] : 0ll;
+    const long long ds_a = (flags & kFlagDs) ? dsp[a] : 0ll;
     // strategy of the canonical mask from the snapshot regrets (node_strategy)
     float sum_r = 0.0f;
 #pragma unroll
@@ -95,16 +97,22 @@ __device__ __forceinline__ void apply_rows(const GameParams& G, const TableView&
     if (G.cfr_plus) r = (r < 0.0f) ? 0.0f : r;
     regp[a] = r;
     ssp[a] = __fadd_rn(s_a, __double2float_rn(__dmul_rn(__dmul_rn((double)dsv, s32), w)));
-    dap[a] = 0;
-    if (flags & 1u) dsp[a] = 0;
+    if (flags & kFlagDa) dap[a] = 0;
+    if (flags & kFlagDs) dsp[a] = 0;
     if (a == 0) {
       *row_visits(tv, slot) += cnt >> 32;
       *row_cnt(tv, slot) = 0;
       *row_su(tv, slot) = 0;
       *row_flags(tv, slot) = 0;
+      wide += (flags & (kFlagDa | kFlagDs)) != 0;
     }
   }
-  if (leader) tv.n_touched[(uid + 1) & 1] = 0;
+  wide = __reduce_add_sync(0xFFFFFFFFu, wide);
+  if ((threadIdx.x & 31) == 0 && wide) atomicAdd(tv.n_touched + 2 + (uid & 1), wide);
+  if (leader) {
+    tv.n_touched[(uid + 1) & 1] = 0;
+    tv.n_touched[2 + ((uid + 1) & 1)] = 0;
+  }
 }
 
 __global__ void __launch_bounds__(256) k_apply(const GameParams G, const TableView tv,
@@ -362,6 +370,7 @@ struct mccfr_handle {
   long long launches = 0;
   double traverse_ms = 0, apply_ms = 0, last_traverse_ms = 0, last_apply_ms = 0;
   long long touched_last = 0;
+  long long wide_last = 0;  // of those, rows whose second line was folded
   int sticky_err = 0;
   std::string last_error;
   size_t persist_prev = 0;
@@ -1194,10 +1203,12 @@ int mccfr_step(mccfr_handle* h, long long iteration, int player, int batch, mccf
     h->traverse_ms += t1;
     h->apply_ms += t2;
     h->launches++;
-    unsigned nt[2] = {0, 0};
+    unsigned nt[4] = {0, 0, 0, 0};
     cudaMemcpy(nt, h->tv.n_touched, sizeof(nt), cudaMemcpyDeviceToHost);
-    // the apply kernel resets the other parity's counter, not this one
-    h->touched_last = nt[(uint32_t)((iteration - 1) * h->cfg.num_players + player) & 1];
+    // the apply kernel resets the other parity's counters, not this one's
+    const uint32_t par = (uint32_t)((iteration - 1) * h->cfg.num_players + player) & 1;
+    h->touched_last = nt[par];
+    h->wide_last = nt[2 + par];
     rc = check_device_error(h);
   }
   if (rc == MCCFR_OK && trace) {
@@ -1239,9 +1250,11 @@ int mccfr_train(mccfr_handle* h, long long iters, int batch, int verbose, const 
       if (i + 1 == iters) {
         // rows touched by this iteration's last player-update (its parity's counter
         // is reset only by the next update's apply)
-        unsigned nt[2] = {0, 0};
+        unsigned nt[4] = {0, 0, 0, 0};
         CK(cudaMemcpy(nt, h->tv.n_touched, sizeof(nt), cudaMemcpyDeviceToHost));
-        h->touched_last = nt[(uint32_t)((base + i) * np + np - 1) & 1];
+        const uint32_t par = (uint32_t)((base + i) * np + np - 1) & 1;
+        h->touched_last = nt[par];
+        h->wide_last = nt[2 + par];
       }
     }
     h->launches += h->cfg.num_players;
@@ -1291,6 +1304,7 @@ int mccfr_get_stats(mccfr_handle* h, mccfr_stats* out) {
   out->last_apply_ms = h->last_apply_ms;
   out->device_error = h->sticky_err;
   out->touched_last = h->touched_last;
+  out->wide_rows_last = (int32_t)h->wide_last;
   out->rows_used = -1;  // filled by mccfr_export_rows callers; counting needs a table scan
   return MCCFR_OK;
 }
@@ -1450,6 +1464,7 @@ int mccfr_import_tables(mccfr_handle* h, const float* regrets, const float* stra
   cudaFree(ds);
   if (!rc) {
     h->touched_last = 0;
+    h->wide_last = 0;
     rc = check_device_error(h);
   }
   return rc;
@@ -1607,6 +1622,7 @@ int mccfr_load_checkpoint_v2(mccfr_handle* h, const char* path) {
   if (!rc) {
     h->iterations_done = iters;
     h->touched_last = 0;
+    h->wide_last = 0;
   }
   return rc;
 }
@@ -2222,6 +2238,7 @@ int mccfr_subgame_reset(mccfr_handle* h, const mccfr_config* cfg, const mccfr_su
   h->round_player = 0;
   h->traverse_ms = h->apply_ms = h->last_traverse_ms = h->last_apply_ms = 0;
   h->touched_last = 0;
+  h->wide_last = 0;
   h->sticky_err = 0;
   h->last_error.clear();
   return MCCFR_OK;

@@ -274,6 +274,7 @@ __device__ __forceinline__ int es_step(const GameParams& G, const TableView& tv,
         return 2;
       }
       EsFrame& F = fr.at(L.sp++);
+      mark_deltas(tv, (unsigned long long)slot);
       F.st = cur;
       node_strategy(reg, vm, F.strat);
       F.vh = 0.0f;

@@ -419,6 +419,7 @@ k_level_back(const GameParams G, const TableView tv, const Sched* __restrict__ s
     const uint32_t vm = m.w;
     if (!vm) continue;
     const unsigned long long slot = m.x;
+    mark_deltas(tv, slot);
     float vh = 0.0f;
     uint32_t o = m.z;
 #pragma unroll

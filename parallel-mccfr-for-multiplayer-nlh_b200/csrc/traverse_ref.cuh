@@ -536,6 +536,7 @@ k_traverse_ref(const GameParams G, const TableView tv, const DealRec* __restrict
     if (touch_row(tv, slot, uid, vm)) {
       atomicAdd(row_cnt(tv, slot), (1ull << 32) | 1ull);
       atomicAdd(row_su(tv, slot), (unsigned long long)fu);
+      mark_deltas(tv, slot);
       atomicAdd(row_da(tv, slot) + s, (unsigned long long)(dsamp + fu));
     } else {
       // Mask differs from the row's canonical one (an FNV slot shared by states

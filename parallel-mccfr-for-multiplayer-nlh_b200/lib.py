@@ -64,7 +64,7 @@ class Stats(Structure):
         ("hand_evals", c_int64), ("rows_used", c_int64), ("table_capacity", c_int64),
         ("touched_last", c_int64), ("traverse_ms", c_double), ("apply_ms", c_double),
         ("last_traverse_ms", c_double), ("last_apply_ms", c_double), ("device_error", c_int32),
-        ("reserved", c_int32 * 7),
+        ("wide_rows_last", c_int32), ("reserved", c_int32 * 6),
     ]
 
 

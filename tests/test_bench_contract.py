@@ -52,11 +52,11 @@ def test_apply_roofline():
     sys.path.insert(0, str(ROOT))
     import bench as b
 
-    s0 = SimpleNamespace(apply_ms=1.0, touched_last=0)
-    s1 = SimpleNamespace(apply_ms=11.0, touched_last=1_000_000)
+    s0 = SimpleNamespace(apply_ms=1.0, touched_last=0, wide_rows_last=0)
+    s1 = SimpleNamespace(apply_ms=11.0, touched_last=1_000_000, wide_rows_last=250_000)
     a = b.apply_roofline(s0, s1, 2, 6000.0)
     assert a["kernel_ms_per_launch"] == 5.0
-    assert a["achieved"] == pytest.approx(1_000_000 * 516 / 0.005 / 1e9)
+    assert a["achieved"] == pytest.approx((1_000_000 * 260 + 250_000 * 256) / 0.005 / 1e9)
     assert a["frac"] == pytest.approx(a["achieved"] / 6000.0)
 
 
