@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--curve", type=str, default="", metavar="I1,I2,...",
                     help="only: time single iterations at these points of one training run (one JSON line)")
     ap.add_argument("--form", type=int, default=-1, help="traversal form (0 auto, 1 lanes, 2 levels)")
+    ap.add_argument("--c4-only", type=int, default=0, metavar="LOG2_HANDS",
+                    help="only: the showdown microbench with 2^LOG2_HANDS 7-card hands and as many 6-seat deals "
+                         "(one JSON line; profiling cases)")
     return ap.parse_args()
 
 
@@ -664,6 +667,12 @@ def main():
         dist.init_process_group(backend, timeout=timedelta(seconds=300))
     cfg.device = local_rank
     table = L.hand_table()
+    if args.c4_only:
+        if rank == 0:
+            n = 1 << args.c4_only
+            print(json.dumps({"c4_showdown": c4_showdown(m, L, table, total=n, chunk=min(n, 1 << 24), deals6=n)}),
+                  flush=True)
+        return
     if args.curve:
         if rank == 0:
             pts = [int(x) for x in args.curve.split(",") if x.strip()]

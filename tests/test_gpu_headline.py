@@ -153,13 +153,18 @@ def test_fp32_order_within_tolerance_over_updates(hand_table, case):
     the device's rows are handed to the oracle in FP32 mode, which adds every
     delta as an FP32 value in traversal order (the reference's atomics,
     cfr_gpu.cu:788, 1006-1007) instead of summing exactly in fixed point; after
-    the update both tables hold the same keys and their regrets and strategy
-    sums agree within 1e-5 relative."""
+    the update both tables hold the same keys, and every row's regrets and
+    strategy sums agree within 1e-5 of the row's largest magnitude (at least 1):
+    |a - b| <= 1e-5 * max(max_row |b|, 1).  The bound is per row because a value
+    that is the cancellation of large deltas carries the FP32 order's own
+    rounding (about 2^-12 chips for 6-max deltas of thousands of chips), which no
+    elementwise relative bound can hold near zero; the elementwise worst case is
+    reported beside it."""
     cfg, batch, _ = fp32_cases()[case]
     tr = trainer(cfg, hand_table)
     orc = binding.Oracle(cfg, hand_table)
     orc.set_float_mode(True)
-    worst = 0.0
+    worst_row, worst_elem = 0.0, 0.0
     for it in (1, 2):
         for p in range(cfg.num_players):
             before = tr.export_rows()
@@ -171,9 +176,14 @@ def test_fp32_order_within_tolerance_over_updates(hand_table, case):
             assert np.array_equal(g["visits"], o["visits"])
             for f in ("regrets", "strategy_sum"):
                 a, b = g[f].astype(np.float64), o[f].astype(np.float64)
-                err = np.abs(a - b) / np.maximum(np.abs(b), 1.0)
-                worst = max(worst, float(err.max()) if err.size else 0.0)
+                if not a.size:
+                    continue
+                scale = np.maximum(np.abs(b).max(axis=1, keepdims=True), 1.0)
+                err = np.abs(a - b) / scale
+                worst_row = max(worst_row, float(err.max()))
+                worst_elem = max(worst_elem, float((np.abs(a - b) / np.maximum(np.abs(b), 1.0)).max()))
                 assert np.all(err <= 1e-5), (it, p, f, float(err.max()))
-    assert worst > 0.0  # the two summation orders do differ
+    print(f"fp32 order: worst per-row relative difference {worst_row:.3g}, elementwise {worst_elem:.3g}")
+    assert worst_row > 0.0  # the two summation orders do differ
     tr.close()
     orc.close()

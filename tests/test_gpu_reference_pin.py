@@ -7,9 +7,11 @@ numbers were drawn:
 
 * its own 6-max game never learns (every player takes the passive fallback,
   24 decisions and 3 street changes reach the depth-20 cut, whose value is 0):
-  all regrets stay exactly 0 in both, every touched slot averages to the uniform
-  strategy over its legal actions in both, and the slots' visit counts (uniform
-  deals through the same buckets and keys) agree within Poisson error;
+  all regrets stay exactly 0 in both, the touched slots average to the uniform
+  strategy over their legal actions in both (all but the few slots that FNV
+  collisions share between info sets of different legal masks, in equal
+  shares), and the slots' visit counts (uniform deals through the same buckets
+  and keys) agree within Poisson error;
 * heads-up, where it learns: aggregate figures (touched slots, the strategy mass
   and positive-regret mass of each action slot) differ from this trainer's by
   no more than this trainer's own figures differ between seeds.
@@ -53,21 +55,26 @@ def our_rows(table, players, iters, batch, seed=42):
             "strategy_sum": r["strategy_sum"][live]}
 
 
-def uniform_over_legal(ssum):
-    """Every row's non-zero strategy sums are equal: a uniform average strategy."""
+def uniform_share(ssum):
+    """Fraction of rows whose non-zero strategy sums are all equal: a uniform
+    average strategy.  A slot shared by info sets with different legal masks (an
+    FNV collision) sums different uniform strategies, so a few rows are not."""
     s = ssum.astype(np.float64)
     hi = np.where(s > 0, s, -np.inf).max(1)
     lo = np.where(s > 0, s, np.inf).min(1)
-    return np.all(s >= 0) and np.all((hi - lo) <= 1e-5 * hi)
+    assert np.all(s >= 0)
+    return float(np.mean((hi - lo) <= 1e-5 * hi))
 
 
 def test_reference_six_max_never_learns_in_either(hand_table, hand_table_file, tmp_path):
     batch = 1 << 18
     ref = reference_rows(tmp_path, hand_table_file, 6, 1, batch)
     ours = our_rows(hand_table, 6, 1, batch)
+    shares = []
     for d in (ref, ours):
         assert np.all(d["regrets"] == 0)
-        assert uniform_over_legal(d["strategy_sum"])
+        shares.append(uniform_share(d["strategy_sum"]))
+    assert min(shares) > 0.99 and abs(shares[0] - shares[1]) < 0.002, shares
     # one iteration, weight 1: a slot's strategy sum is its visit count
     ca = dict(zip(ref["slots"].tolist(), ref["strategy_sum"].sum(1).round().astype(np.int64).tolist()))
     cb = dict(zip(ours["slots"].tolist(), ours["strategy_sum"].sum(1).round().astype(np.int64).tolist()))
