@@ -471,7 +471,7 @@ def serving_sweep(m, L, table, rates=(10, 30, 100, 300, 1000), n_requests=48) ->
         reqs = [sv.make_request(rng, i) for i in range(n_requests)]
         for r, a in zip(reqs, sv.poisson_arrivals(rng, n_requests, rate)):
             r.arrival = float(a)
-        srv = sv.ReSolveServer(owner, hbm_budget=32 << 30, traversals=1024)
+        srv = sv.ReSolveServer(owner, hbm_budget=32 << 30, traversals=1024, retire_workers=2)
         res = srv.run(reqs)
         line = {**sv.summarize(res), "rounds": srv.rounds, "tables_reused": srv.reused,
                 **{k: round(v, 3) for k, v in srv.timing.items()}}
@@ -488,8 +488,9 @@ def serving_sweep(m, L, table, rates=(10, 30, 100, 300, 1000), n_requests=48) ->
                        "Dirichlet(0.5) ranges, 3-6 sizes drawn (at most 5 kept: fold, check/call, the sizes and "
                        "all-in fill the 8 action slots of a row) + all-in, 100BB stacks, seed 4. Budget unit: "
                        "iterations of the one-traversal-per-player form, log-uniform [2e3,5e4] = traversals per "
-                       "player, spent 1024 per player-update. plain_trainer: the same trace served one request "
-                       "at a time by train() in arrival order")
+                       "player, spent 1024 per player-update; strategies exported by 2 retire workers beside the "
+                       "rounds. plain_trainer: the same trace served one request at a time by train() in arrival "
+                       "order")
     return out
 
 
@@ -711,6 +712,13 @@ def main():
     launches = args.steps * cfg.num_players
     trav_ms = s1.traverse_ms - s0.traverse_ms
 
+    levels = None
+    if cfg.sampling == 1 and cfg.traversal_form != 1:
+        try:
+            levels = tr.level_counts()
+        except Exception as e:  # noqa: BLE001
+            levels = {"error": str(e)}
+
     # the table after the timed region: the oracle's CPU baseline walks the same
     # trees as the device's next update (taken before the e2e steps run it)
     cpu_rows = None
@@ -765,6 +773,7 @@ def main():
         "table": {"rows_used": rows_used, "capacity": int(s1.table_capacity),
                   "load": rows_used / max(1, s1.table_capacity), "record_bytes": 256,
                   "span_gb": s1.table_capacity * 256 / 1e9},
+        "levels_last_update": levels,
         "node_visits_per_s": visits / (ms / 1e3) * world,
         "hand_evals_per_s": (s1.hand_evals - s0.hand_evals) / (ms / 1e3) * world,
     }

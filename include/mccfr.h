@@ -289,6 +289,14 @@ int mccfr_eval7(mccfr_handle* h, const uint8_t* cards, uint16_t* ranks, size_t n
 int mccfr_eval7_device(mccfr_handle* h, const uint8_t* dev_cards,
                        uint16_t* dev_ranks, size_t n, float* ms);
 
+/* The level-synchronous form's counts of the handle's last external-sampling
+   update: seeds[L] (level 0: the update's traversals) and updating-player
+   nodes[L] reached from level L, for L < min(cap, *levels), and the seeds left
+   to the depth-first walk because the buffers were full.  *levels = 0 before
+   the first such update.  No reference counterpart (a tuning aid). */
+int mccfr_level_counts(mccfr_handle* h, uint32_t* seeds, uint32_t* nodes, int cap, int* levels,
+                       uint32_t* deferred);
+
 /* ---- showdown microbenchmark ---------------------------------------------
    No reference counterpart as entry points; they time the gathers of the
    reference's rank chains and showdown (cfr_gpu.cu:114-150, 694-753) alone.

@@ -361,6 +361,7 @@ struct mccfr_handle {
   void* d_level = nullptr;
   size_t level_bytes = 0;
   int level_batch = 0;  // batch the buffers were sized for
+  int level_last_batch = 0;  // traversals of the last update enqueued in the level form
   LevelBufs lb{};
   int grid_expand = 0, grid_back = 0, grid_dfs = 0;  // resident blocks on this handle's device
   // graph of one iteration
@@ -681,6 +682,7 @@ int ensure_levels(mccfr_handle* h, int batch) {
 // returned bottom up.
 int enqueue_levels(mccfr_handle* h, int batch, float rscale) {
   const LevelBufs& lb = h->lb;
+  h->level_last_batch = batch;
   CK(cudaMemsetAsync(lb.ctl, 0, sizeof(LevelCtl), h->stream));
   for (int L = 0; L < lb.nlev; ++L)
     k_level_expand<128, 1><<<h->grid_expand, 128, 0, h->stream>>>(h->gp, h->tv, h->d_deals, h->d_sched, batch, lb,
@@ -1680,6 +1682,25 @@ int mccfr_eval7(mccfr_handle* h, const uint8_t* cards, uint16_t* ranks, size_t n
   cudaFree(dc);
   cudaFree(dr);
   return rc;
+}
+
+int mccfr_level_counts(mccfr_handle* h, uint32_t* seeds, uint32_t* nodes, int cap, int* levels,
+                       uint32_t* deferred) {
+  if (!h || !levels || cap < 0 || (cap && (!seeds || !nodes))) return MCCFR_ERR_INVALID_ARG;
+  *levels = 0;
+  if (deferred) *deferred = 0;
+  if (!h->d_level) return MCCFR_OK;
+  CK(cudaSetDevice(h->device));
+  LevelCtl c;
+  CK(cudaMemcpyAsync(&c, h->lb.ctl, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  *levels = h->lb.nlev;
+  for (int L = 0; L < h->lb.nlev && L < cap; ++L) {
+    seeds[L] = L == 0 ? (uint32_t)h->level_last_batch : c.seed_count[L];
+    nodes[L] = c.node_count[L];
+  }
+  if (deferred) *deferred = c.deferred;
+  return MCCFR_OK;
 }
 
 int mccfr_deal_eval7(mccfr_handle* h, uint32_t stream, size_t n, uint16_t* dev_ranks, float* ms) {

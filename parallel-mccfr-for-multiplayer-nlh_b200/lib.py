@@ -140,6 +140,7 @@ SIGNATURES = {
     "mccfr_export_rows": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, POINTER(c_size_t)]),
     "mccfr_table_digest": (c_int, [c_void_p, c_void_p, c_void_p]),
     "mccfr_deal_eval7": (c_int, [c_void_p, c_uint32, c_size_t, c_void_p, POINTER(c_float)]),
+    "mccfr_level_counts": (c_int, [c_void_p, c_void_p, c_void_p, c_int, POINTER(c_int), POINTER(c_uint32)]),
     "mccfr_showdown_masks": (c_int, [c_void_p, c_longlong, c_int, c_size_t, c_void_p, POINTER(c_float)]),
     "mccfr_export_tables": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),
     "mccfr_import_tables": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),

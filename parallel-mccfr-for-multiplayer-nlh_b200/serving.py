@@ -15,6 +15,8 @@ from __future__ import annotations
 import math
 import threading
 import time
+from concurrent.futures import FIRST_COMPLETED, ThreadPoolExecutor
+from concurrent.futures import wait as wait_futures
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -150,11 +152,17 @@ class ReSolveServer:
     memory with every pooled table freed) is refused with an error result
     instead of blocking the queue.  round_fn and create_fn
     replace the device round (batch_round) and the table creation, so the loop's
-    host logic can run against stand-ins."""
+    host logic can run against stand-ins.
+
+    retire_workers > 0 moves retiring off the round loop: a finished request's
+    strategy is exported (a counting pass, a compaction and a copy on its own
+    handle's stream, then the host sort) by a worker thread while the loop goes
+    on running rounds for the others; its table counts against the budget until
+    the export is done and then returns to the pool.  0 retires in the loop."""
 
     def __init__(self, rank_table_owner: GPUCFRTrainer, hbm_budget: int = 16 << 30, max_active: int = 64,
                  traversals: int = 256, tuning: dict | None = None, free_memory=None, round_fn=None,
-                 create_fn=None):
+                 create_fn=None, retire_workers: int = 0):
         self.owner = rank_table_owner
         self.hbm_budget = int(hbm_budget)
         self.max_active = min(64, int(max_active))
@@ -172,6 +180,7 @@ class ReSolveServer:
         self._create = create_fn or self._create_subgame
         self._lock = threading.Lock()
         self._withdrawn: set[int] = set()
+        self.retire_workers = int(retire_workers)
 
     def cancel(self, rid: int) -> None:
         with self._lock:
@@ -243,7 +252,41 @@ class ReSolveServer:
             self.cancelled += 1
             results.append(Result(req.rid, req.arrival, admitted, time.perf_counter() - t0, *none, cancelled=True))
 
-        while pending or queue or active:
+        def export(s: Solve):
+            keys, probs = s.trainer.strategy_arrays()
+            return keys, probs, time.perf_counter() - t0
+
+        workers = ThreadPoolExecutor(self.retire_workers) if self.retire_workers > 0 else None
+        retiring: list[tuple] = []  # (future, solve) of exports in flight
+
+        def collect(wait: bool) -> int:
+            """Books the exports that are done (waiting for one when `wait`);
+            returns the device bytes their tables free for admission."""
+            freed = 0
+            if wait and retiring and not any(f.done() for f, _ in retiring):
+                wait_futures([f for f, _ in retiring], return_when=FIRST_COMPLETED)
+            for item in [x for x in retiring if x[0].done()]:
+                f, s = item
+                keys, probs, done_at = f.result()
+                results.append(Result(s.req.rid, s.req.arrival, s.admitted, done_at, keys, probs))
+                with self._lock:
+                    self.pool.setdefault(s.req.table_log2, []).append(s.trainer)
+                freed += table_bytes(s.req)
+                retiring.remove(item)
+            return freed
+
+        try:
+            self._serve(pending, queue, active, held, results, t0, none, withdraw, export, workers, retiring,
+                        collect, realtime)
+        finally:
+            if workers is not None:
+                workers.shutdown(wait=True)
+        return results
+
+    def _serve(self, pending, queue, active, held, results, t0, none, withdraw, export, workers, retiring, collect,
+               realtime) -> None:
+        while pending or queue or active or retiring:
+            held -= collect(wait=False)
             now = time.perf_counter() - t0
             while pending and (not realtime or pending[0].arrival <= now):
                 queue.append(pending.pop(0))
@@ -256,6 +299,9 @@ class ReSolveServer:
                 active.append(self._start(req, time.perf_counter() - t0))
                 held += table_bytes(req)
             self.timing["admit_s"] += time.perf_counter() - ta
+            if not active and retiring:
+                held -= collect(wait=True)  # tables in export come back before anything is refused
+                continue
             if not active and queue:
                 # nothing runs and no pooled table is left to free, yet the head of
                 # the queue does not fit: it never will, so it is refused rather
@@ -283,15 +329,17 @@ class ReSolveServer:
                     self.pool.setdefault(s.req.table_log2, []).append(s.trainer)
                     held -= table_bytes(s.req)
                 elif s.updates_done >= s.updates_needed:
-                    keys, probs = s.trainer.strategy_arrays()
-                    results.append(Result(s.req.rid, s.req.arrival, s.admitted, time.perf_counter() - t0, keys, probs))
-                    self.pool.setdefault(s.req.table_log2, []).append(s.trainer)  # kept for the next request
-                    held -= table_bytes(s.req)
+                    if workers is not None:
+                        retiring.append((workers.submit(export, s), s))  # its table is held until exported
+                    else:
+                        keys, probs, done_at = export(s)
+                        results.append(Result(s.req.rid, s.req.arrival, s.admitted, done_at, keys, probs))
+                        self.pool.setdefault(s.req.table_log2, []).append(s.trainer)  # kept for the next request
+                        held -= table_bytes(s.req)
                 else:
                     still.append(s)
-            active = still
+            active[:] = still
             self.timing["retire_s"] += time.perf_counter() - tz
-        return results
 
 
 def updates_for(req: Request, traversals: int) -> int:

@@ -211,6 +211,17 @@ class GPUCFRTrainer:
         m = n.value
         return {"keys": keys[:m], "regrets": reg[:m], "strategy_sum": ssum[:m], "visits": vis[:m]}
 
+    def level_counts(self) -> dict:
+        """Per-level seeds and updating-player nodes of the last external-sampling
+        update in the level-synchronous form (mccfr_level_counts)."""
+        seeds = np.zeros(64, np.uint32)
+        nodes = np.zeros(64, np.uint32)
+        n, deferred = ctypes.c_int(), ctypes.c_uint32()
+        L.check(self._lib.mccfr_level_counts(self._h, L.ptr(seeds), L.ptr(nodes), 64, byref(n), byref(deferred)),
+                self._h)
+        k = n.value
+        return {"seeds": seeds[:k].tolist(), "nodes": nodes[:k].tolist(), "deferred": int(deferred.value)}
+
     def digest(self) -> tuple[int, int]:
         """(checksum, occupied rows) of the table, computed on the device
         (mccfr_table_digest): equal for tables with the same rows."""

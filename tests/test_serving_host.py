@@ -2,6 +2,7 @@
 from __future__ import annotations
 
 import importlib
+import time
 
 import numpy as np
 import pytest
@@ -227,3 +228,38 @@ def test_budget_counts_traversals_per_player():
     assert sv.updates_for(reqs[0], 256) == 4
     reqs[0].budget = 1000
     assert sv.updates_for(reqs[0], 256) == 4  # rounded up
+
+
+def test_retire_workers_export_while_rounds_go_on():
+    """With a retire worker a finished request's export runs beside the rounds of
+    the others: rounds happen while an export is in flight, every request still
+    gets its strategy, and the exported tables return to the pool for reuse."""
+    import threading
+
+    reqs = _same_size_requests(4)
+    reqs[0].budget = 256  # finishes after one round per player, long before the others
+    exporting = threading.Event()
+    rounds_while_exporting = [0]
+
+    class SlowExport(_FakeSolver):
+        def strategy_arrays(self):
+            exporting.set()
+            time.sleep(0.2)
+            exporting.clear()
+            return super().strategy_arrays()
+
+    def round_fn(trainers, traversals, tuning):
+        if exporting.is_set():
+            rounds_while_exporting[0] += 1
+        time.sleep(0.01)
+
+    # room for three tables: the fourth request waits for an exported table
+    srv = sv.ReSolveServer(None, hbm_budget=3 * sv.table_bytes(reqs[0]), max_active=3,
+                           free_memory=lambda: 100 << 30, traversals=256, round_fn=round_fn,
+                           create_fn=lambda cfg, req: SlowExport(), retire_workers=1)
+    res = {r.rid: r for r in srv.run(reqs, realtime=False)}
+    assert set(res) == {r.rid for r in reqs}
+    assert all(r.keys.tolist() == [7] and not r.error and not r.cancelled for r in res.values())
+    assert rounds_while_exporting[0] > 0
+    assert srv.reused >= 1  # the fourth request ran on the table that came back from an export
+    srv.close()
