@@ -59,14 +59,19 @@ constexpr int kRefBlock = 128;
 __device__ __forceinline__ void apply_rows(const GameParams& G, const TableView& tv, const Sched* sched, double rinv,
                                            unsigned group, unsigned ngroups, bool leader) {
   const uint32_t uid = update_id(sched, G.N);
-  const unsigned n = tv.n_touched[uid & 1];
+  const unsigned n_narrow = tv.n_touched[uid & 1];
+  const unsigned n = n_narrow + tv.n_touched[2 + (uid & 1)];
   const double w = G.lcfr ? (double)(float)sched->iteration : 1.0;
   const double s32 = 2.3283064365386962890625e-10;  // 2^-32
   const int a = threadIdx.x & 7;
   const unsigned gmask = 0xFFu << (threadIdx.x & 24);
-  unsigned wide = 0;  // rows whose second line was folded too (counted by lane 0 of each group)
+  unsigned wide_rows = 0;  // rows whose second line was folded too (counted by lane 0 of each group)
   for (unsigned i = group; i < n; i += ngroups) {
-    const unsigned long long slot = tv.touched[i];
+    // the narrow list's rows were first touched by sampled opponents and hold
+    // no regret accumulators unless a flag says so (a shared key); the wide
+    // list's rows always do, so both their lines are read at once
+    const bool listed_wide = i >= n_narrow;
+    const unsigned long long slot = listed_wide ? tv.touched_wide[i - n_narrow] : tv.touched[i];
     const uint32_t m = (uint32_t)(*row_tag(tv, slot) & 0xFF);
     const unsigned long long cnt = *row_cnt(tv, slot);
     const long long canon = (long long)(cnt & 0xFFFFFFFFull);
@@ -78,8 +83,10 @@ __device__ __forceinline__ void apply_rows(const GameParams& G, const TableView&
     long long* dsp = reinterpret_cast<long long*>(row_ds(tv, slot));
     const float r_a = regp[a];
     const float s_a = ssp[a];
-    // a row visited only by sampled opponents has nothing on its second line
-    const long long da_a = (flags & kFlagDa) ? dap[a] : 0ll;
+    long long da_a = 0;
+    if (listed_wide) da_a = dap[a];
+    const bool has_da = listed_wide || (flags & kFlagDa);
+    if (!listed_wide && (flags & kFlagDa)) da_a = dap[a];
     const long long ds_a = (flags & kFlagDs) ? dsp[a] : 0ll;
     // strategy of the canonical mask from the snapshot regrets (node_strategy)
     float sum_r = 0.0f;
@@ -97,21 +104,23 @@ __device__ __forceinline__ void apply_rows(const GameParams& G, const TableView&
     if (G.cfr_plus) r = (r < 0.0f) ? 0.0f : r;
     regp[a] = r;
     ssp[a] = __fadd_rn(s_a, __double2float_rn(__dmul_rn(__dmul_rn((double)dsv, s32), w)));
-    if (flags & kFlagDa) dap[a] = 0;
+    if (has_da) dap[a] = 0;
     if (flags & kFlagDs) dsp[a] = 0;
     if (a == 0) {
       *row_visits(tv, slot) += cnt >> 32;
       *row_cnt(tv, slot) = 0;
       *row_su(tv, slot) = 0;
       *row_flags(tv, slot) = 0;
-      wide += (flags & (kFlagDa | kFlagDs)) != 0;
+      wide_rows += (has_da || (flags & kFlagDs)) ? 1u : 0u;
     }
   }
-  wide = __reduce_add_sync(0xFFFFFFFFu, wide);
-  if ((threadIdx.x & 31) == 0 && wide) atomicAdd(tv.n_touched + 2 + (uid & 1), wide);
+  wide_rows = __reduce_add_sync(0xFFFFFFFFu, wide_rows);
+  if ((threadIdx.x & 31) == 0 && wide_rows) atomicAdd(tv.n_touched + 4 + (uid & 1), wide_rows);
   if (leader) {
-    tv.n_touched[(uid + 1) & 1] = 0;
-    tv.n_touched[2 + ((uid + 1) & 1)] = 0;
+    const uint32_t next = (uid + 1) & 1;
+    tv.n_touched[next] = 0;
+    tv.n_touched[2 + next] = 0;
+    tv.n_touched[4 + next] = 0;
   }
 }
 
@@ -603,8 +612,8 @@ int level_count(const mccfr_handle* h) {
 }
 
 // Node and seed buffers for updates of `batch` traversals: 2^level_log2 node
-// records (default: 64 per traversal, 2^18..2^26) and 8 seeds per node (at
-// least the batch and a margin).  A smaller allocation is tried when the
+// records of 80 B (default: 64 per traversal, 2^18..2^26) and 8 seeds of 8 B
+// per node (at least the batch and a margin).  A smaller allocation is tried when the
 // device is short of memory; any size gives the same rows.
 int ensure_levels(mccfr_handle* h, int batch) {
   const int nlev = level_count(h);
@@ -631,7 +640,7 @@ int ensure_levels(mccfr_handle* h, int batch) {
   for (;; --lg) {
     const unsigned long long nodes = 1ull << lg;
     const unsigned long long seeds = std::max(8ull * nodes, (unsigned long long)batch + (1ull << 20));
-    const size_t bytes = nodes * (sizeof(EsState) + sizeof(uint4)) + seeds * 12 + sizeof(LevelCtl) + 256;
+    const size_t bytes = nodes * (sizeof(EsState) + sizeof(uint4)) + seeds * 8 + sizeof(LevelCtl) + 256;
     const cudaError_t e = cudaMalloc(&h->d_level, bytes);
     if (e == cudaSuccess) {
       char* p = static_cast<char*>(h->d_level);
@@ -640,8 +649,6 @@ int ensure_levels(mccfr_handle* h, int batch) {
       h->lb.meta = reinterpret_cast<uint4*>(p);
       p += nodes * sizeof(uint4);
       h->lb.child = reinterpret_cast<uint32_t*>(p);
-      p += seeds * 4;
-      h->lb.cstrat = reinterpret_cast<float*>(p);
       p += seeds * 4;
       h->lb.value = reinterpret_cast<float*>(p);
       p += seeds * 4;
@@ -660,7 +667,7 @@ int ensure_levels(mccfr_handle* h, int batch) {
   if (!h->grid_expand) {
     int sms = 0, per = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_level_expand<128, 1>, 128, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_level_expand<128, 1, false>, 128, 0));
     h->grid_expand = std::max(1, per) * sms;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_level_back<256>, 256, 0));
     h->grid_back = std::max(1, per) * sms;
@@ -684,9 +691,11 @@ int enqueue_levels(mccfr_handle* h, int batch, float rscale) {
   const LevelBufs& lb = h->lb;
   h->level_last_batch = batch;
   CK(cudaMemsetAsync(lb.ctl, 0, sizeof(LevelCtl), h->stream));
-  for (int L = 0; L < lb.nlev; ++L)
-    k_level_expand<128, 1><<<h->grid_expand, 128, 0, h->stream>>>(h->gp, h->tv, h->d_deals, h->d_sched, batch, lb,
-                                                                  L, h->d_counters);
+  k_level_expand<128, 1, true><<<h->grid_expand, 128, 0, h->stream>>>(h->gp, h->tv, h->d_deals, h->d_sched, batch,
+                                                                      lb, 0, h->d_counters);
+  for (int L = 1; L < lb.nlev; ++L)
+    k_level_expand<128, 1, false><<<h->grid_expand, 128, 0, h->stream>>>(h->gp, h->tv, h->d_deals, h->d_sched,
+                                                                         batch, lb, L, h->d_counters);
   CK(cudaGetLastError());
   k_level_dfs<128, 2, 1><<<h->grid_dfs, 128, 2 * 128 * sizeof(EsFrame), h->stream>>>(
       h->gp, h->tv, h->d_deals, h->d_sched, batch, rscale, lb, h->d_counters);
@@ -1052,13 +1061,14 @@ int mccfr_create(const mccfr_config* cfg, mccfr_handle** out) {
   // Table rows, the touched list and small counters in one allocation.
   h->cap = 1ull << cfg->table_log2;
   const unsigned long long C = h->cap;
-  const size_t bytes_rows = C * kRowBytes, bytes_touch = C * 4, bytes_misc = 256;
+  const size_t bytes_rows = C * kRowBytes, bytes_touch = C * 8, bytes_misc = 256;  // two touched lists
   h->block_bytes = bytes_rows + bytes_touch + bytes_misc;
   CKC(cudaMalloc(&h->d_block, bytes_rows + bytes_touch + bytes_misc));
   CKC(cudaMemset(h->d_block, 0, bytes_rows + bytes_touch + bytes_misc));
   char* base = static_cast<char*>(h->d_block);
   h->tv.rows = reinterpret_cast<unsigned char*>(base);
   h->tv.touched = reinterpret_cast<unsigned int*>(base + bytes_rows);
+  h->tv.touched_wide = reinterpret_cast<unsigned int*>(base + bytes_rows + C * 4);
   char* misc = base + bytes_rows + bytes_touch;
   h->tv.n_touched = reinterpret_cast<unsigned int*>(misc);
   h->tv.err = reinterpret_cast<int*>(misc + 64);
@@ -1205,12 +1215,12 @@ int mccfr_step(mccfr_handle* h, long long iteration, int player, int batch, mccf
     h->traverse_ms += t1;
     h->apply_ms += t2;
     h->launches++;
-    unsigned nt[4] = {0, 0, 0, 0};
+    unsigned nt[6] = {0, 0, 0, 0, 0, 0};
     cudaMemcpy(nt, h->tv.n_touched, sizeof(nt), cudaMemcpyDeviceToHost);
     // the apply kernel resets the other parity's counters, not this one's
     const uint32_t par = (uint32_t)((iteration - 1) * h->cfg.num_players + player) & 1;
-    h->touched_last = nt[par];
-    h->wide_last = nt[2 + par];
+    h->touched_last = (long long)nt[par] + nt[2 + par];
+    h->wide_last = nt[4 + par];
     rc = check_device_error(h);
   }
   if (rc == MCCFR_OK && trace) {
@@ -1252,11 +1262,11 @@ int mccfr_train(mccfr_handle* h, long long iters, int batch, int verbose, const 
       if (i + 1 == iters) {
         // rows touched by this iteration's last player-update (its parity's counter
         // is reset only by the next update's apply)
-        unsigned nt[4] = {0, 0, 0, 0};
+        unsigned nt[6] = {0, 0, 0, 0, 0, 0};
         CK(cudaMemcpy(nt, h->tv.n_touched, sizeof(nt), cudaMemcpyDeviceToHost));
         const uint32_t par = (uint32_t)((base + i) * np + np - 1) & 1;
-        h->touched_last = nt[par];
-        h->wide_last = nt[2 + par];
+        h->touched_last = (long long)nt[par] + nt[2 + par];
+        h->wide_last = nt[4 + par];
       }
     }
     h->launches += h->cfg.num_players;

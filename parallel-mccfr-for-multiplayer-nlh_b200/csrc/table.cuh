@@ -31,8 +31,11 @@ constexpr unsigned kFlagDs = 1u, kFlagDa = 2u;
 
 struct TableView {
   unsigned char* rows;       // [cap][256]
-  unsigned int* touched;     // [cap]
-  unsigned int* n_touched;   // [4]: touched rows, then rows with a second line to fold, by update-id parity
+  unsigned int* touched;     // [cap] rows first touched by a sampled opponent (first line only, as a rule)
+  unsigned int* touched_wide;  // [cap] rows first touched by an updating-player node (both lines)
+  // [6], each pair by update-id parity: entries of `touched`, of `touched_wide`,
+  // and rows whose second line the apply kernel folded
+  unsigned int* n_touched;
   unsigned long long mask;   // cap - 1
   int log2cap;
   int direct;                // every key is at most cap: key k owns row k-1, no probing
@@ -136,23 +139,43 @@ __device__ __forceinline__ long long table_insert(const TableView& tv, unsigned 
   return -1;
 }
 
+__device__ __forceinline__ void list_row(const TableView& tv, unsigned long long slot, uint32_t uid, bool wide) {
+  if (wide) {
+    const unsigned int i = atomicAdd(tv.n_touched + 2 + (uid & 1), 1u);
+    tv.touched_wide[i] = (unsigned int)slot;
+  } else {
+    const unsigned int i = atomicAdd(tv.n_touched + (uid & 1), 1u);
+    tv.touched[i] = (unsigned int)slot;
+  }
+}
+
 // Marks the row as touched by update `uid`; returns whether `vm` is the
-// update's canonical mask for that row (the first visitor sets it).
+// update's canonical mask for that row (the first visitor sets it).  The row
+// goes to the wide list when the first visitor will write regret accumulators.
 __device__ __forceinline__ bool touch_row(const TableView& tv, unsigned long long slot, uint32_t uid,
-                                          uint32_t vm) {
+                                          uint32_t vm, bool wide = false) {
   const unsigned long long want = ((unsigned long long)(uid + 1) << 8) | vm;
   unsigned long long* tag = row_tag(tv, slot);
   unsigned long long old = __ldcg(tag);
   if ((old >> 8) != (unsigned long long)(uid + 1)) {
     const unsigned long long r = atomicCAS(tag, old, want);
     if (r == old) {
-      const unsigned int i = atomicAdd(tv.n_touched + (uid & 1), 1u);
-      tv.touched[i] = (unsigned int)slot;
+      list_row(tv, slot, uid, wide);
       return true;
     }
     old = r;
   }
   return (uint32_t)(old & 0xFF) == vm;
+}
+
+// Marks the row as touched by update `uid` without claiming a canonical mask
+// (mask 0: every later visitor takes the direct path), for a visitor that adds
+// its whole regret terms to the per-action accumulators; one atomic whose
+// result only decides the list entry.  Update ids only grow, so the maximum
+// leaves a tag of this update (claimed or not) as it is.
+__device__ __forceinline__ void claim_row(const TableView& tv, unsigned long long slot, uint32_t uid) {
+  const unsigned long long old = atomicMax(row_tag(tv, slot), (unsigned long long)(uid + 1) << 8);
+  if ((old >> 8) < (unsigned long long)(uid + 1)) list_row(tv, slot, uid, true);
 }
 
 // Marks the row's regret accumulators (second line) as holding values in this

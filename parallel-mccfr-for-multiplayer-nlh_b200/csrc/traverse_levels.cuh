@@ -13,24 +13,27 @@
 //              changes and terminals, until it reaches a terminal (the seed's
 //              value) or an updating-player node.  That node gets a record (its
 //              state, row slot, legal mask) and every legal action becomes a
-//              seed of level L+1, with the node's regret-matched probability of
-//              that action.  Lanes take seeds from a per-level counter as they
-//              finish, so a warp keeps its lanes busy whatever the walks' lengths.
+//              seed of level L+1.  Lanes take seeds from a per-level counter as
+//              they finish, so a warp keeps its lanes busy whatever the walks'
+//              lengths.
 //   dfs        seeds that did not fit the buffers (see below) are walked depth
 //              first by the frame-stack walk of k_traverse_es, from the seed.
 //   back(L)    one thread per updating-player node of level L, deepest level
-//              first: it reads its children's values in slot order, adds
-//              fix(v[a]) to the row's per-action accumulators, forms
-//              v_h = sum_a strat[a] * v[a] in the same order as the depth-first
-//              walk, subtracts fix(v_h) (through `su` for the canonical mask) and
-//              hands v_h to its own seed.
+//              first: it regret-matches the node's row (its regrets are a
+//              snapshot the update does not change), reads its children's values,
+//              forms v_h = sum_a strat[a] * v[a] in slot order as the depth-first
+//              walk does, adds fix(v[a]) - fix(v_h) to every legal action's
+//              accumulator and hands v_h to its own seed.  The row is claimed for
+//              the update by one atomic maximum on its tag, with no canonical
+//              mask (the whole regret term goes to the accumulators), so no
+//              thread waits on a compare-and-swap.
 //
 // Every sum that reaches the table is an integer (fixed point) and every draw
 // is keyed by the node's action path, so the rows after an update are
 // bit-identical to the depth-first walk's, whatever the order of the lanes.
 //
 // Buffers.  A level's updating-player nodes and child seeds are appended to
-// two bump-allocated arrays (nodes: 64 B state + 16 B record; seeds: 12 B).  A
+// two bump-allocated arrays (nodes: 64 B state + 16 B record; seeds: 8 B).  A
 // lane checks, when it picks a seed up, that the arrays still have room for
 // the worst case of every lane that may hold a seed meanwhile (one node and
 // num_actions seeds each); a seed that fails the check is marked and left to
@@ -62,7 +65,6 @@ struct LevelBufs {
   EsState* nodes;     // [node_cap] state at the node (aux = traversal index)
   uint4* meta;        // [node_cap] {row slot, own seed, first child seed, legal mask (0: none)}
   uint32_t* child;    // [seed_cap] (node << 3) | action; kSeedDeferred / kSeedInvalid marks
-  float* cstrat;      // [seed_cap] the parent's probability of the seed's action
   float* value;       // [seed_cap] the seed's value for the updating player
   LevelCtl* ctl;
   uint32_t node_cap, seed_cap;
@@ -93,11 +95,11 @@ enum { kLvGoOn = 0, kLvDone = 1, kLvUp = 2 };
 // One step of a seed's walk (the descend branch of es_step): the cheap steps
 // (depth cut, fold win, street change, showdown), then at most one decision
 // node.  An opponent's node is done here; at an updating-player node the walk
-// stops with the node's mask, row slot and regrets.
+// stops with the node's mask and row slot (its regrets are read in back).
 template <int W>
 __device__ __forceinline__ int lv_step(const GameParams& G, const TableView& tv, uint32_t uid, int up, EsState& cur,
                                        const DealRec* D, float& value, uint32_t& vm_out, long long& slot_out,
-                                       float* reg, EsCounts& cnt) {
+                                       EsCounts& cnt) {
   const int N = G.N;
   const uint32_t all_players = (1u << N) - 1;
   for (int guard = 0; guard < 4; ++guard) {
@@ -151,7 +153,6 @@ __device__ __forceinline__ int lv_step(const GameParams& G, const TableView& tv,
   }
   const unsigned long long key = info_key(G, player, hb, bkt, cur.street, cur.abits, cur.path);
   const long long slot = table_insert<W>(tv, key);
-  load_regrets(tv, slot, reg);
   cnt.visits++;
   if (player == up) {
     vm_out = vm;
@@ -159,6 +160,8 @@ __device__ __forceinline__ int lv_step(const GameParams& G, const TableView& tv,
     return kLvUp;
   }
   // sampled opponent: strategy sum, then one action (es_step's opponent branch)
+  float reg[kSlots];
+  load_regrets(tv, slot, reg);
   const U4 d = philox(U4{cur.aux, uid, (uint32_t)cur.path, (uint32_t)(cur.path >> 32) | 0x80000000u}, G.seed_lo,
                       G.seed_hi);
   const int s = sample_action(G, reg, vm, uniform01(d.x));
@@ -180,18 +183,10 @@ __device__ __forceinline__ int lv_step(const GameParams& G, const TableView& tv,
   return kLvGoOn;
 }
 
-// Start state of a seed: the root (level 0) or the parent node's state after the
-// seed's action.
-__device__ __forceinline__ void lv_seed_state(const GameParams& G, const LevelBufs& lb, const DealRec* deals,
-                                              uint32_t seed, uint32_t w, int batch, int up, EsState& cur,
-                                              const DealRec*& D) {
-  if (seed < (uint32_t)batch) {
-    EsLane tmp;
-    es_begin(G, deals + seed, seed, tmp);
-    cur = tmp.cur;
-    D = deals + seed;
-    return;
-  }
+// Start state of a seed of a level below the root: the parent node's state
+// after the seed's action.
+__device__ __forceinline__ void lv_child_state(const GameParams& G, const LevelBufs& lb, const DealRec* deals,
+                                               uint32_t w, int up, EsState& cur, const DealRec*& D) {
   const uint32_t node = (w & ~kSeedDeferred) >> 3;
   const uint4* src = reinterpret_cast<const uint4*>(lb.nodes + node);
   uint4* dst = reinterpret_cast<uint4*>(&cur);
@@ -202,9 +197,19 @@ __device__ __forceinline__ void lv_seed_state(const GameParams& G, const LevelBu
   cur.depth++;
 }
 
+__device__ __forceinline__ void lv_root_state(const GameParams& G, const DealRec* deals, uint32_t t, EsState& cur,
+                                              const DealRec*& D) {
+  EsLane tmp;
+  es_begin(G, deals + t, t, tmp);
+  cur = tmp.cur;
+  D = deals + t;
+}
+
 __device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) { return *(volatile const uint32_t*)p; }
 
-template <int BLOCK, int W>
+// ROOT: level 0, whose seeds are the traversals' roots (built from the deals);
+// deeper levels load their parent's state instead.
+template <int BLOCK, int W, bool ROOT>
 __global__ void __launch_bounds__(BLOCK)
 k_level_expand(const GameParams G, const TableView tv, const DealRec* __restrict__ deals,
                const Sched* __restrict__ sched, int batch, const LevelBufs lb, int L,
@@ -245,7 +250,7 @@ k_level_expand(const GameParams G, const TableView tv, const DealRec* __restrict
           more = false;
         } else {
           seed = B.seed + i;
-          const uint32_t w = L == 0 ? 0u : __ldcg(lb.child + seed);
+          const uint32_t w = ROOT ? 0u : __ldcg(lb.child + seed);
           bool ok = w != kSeedInvalid && !last;
           if (ok) {
             ok = need_nodes + ld_volatile(node_count) <= lb.node_cap &&
@@ -257,9 +262,13 @@ k_level_expand(const GameParams G, const TableView tv, const DealRec* __restrict
             lb.child[seed] = w | kSeedDeferred;
             deferred++;
           } else {
-            if (L == 0) lb.child[seed] = 0u;
-            lv_seed_state(G, lb, deals, seed, w, batch, up, cur, D);
-            if (L == 0) trav++;
+            if (ROOT) {
+              lb.child[seed] = 0u;
+              lv_root_state(G, deals, seed, cur, D);
+              trav++;
+            } else {
+              lv_child_state(G, lb, deals, w, up, cur, D);
+            }
             have = true;
           }
         }
@@ -269,10 +278,9 @@ k_level_expand(const GameParams G, const TableView tv, const DealRec* __restrict
     int r = -1;
     uint32_t vm = 0;
     long long slot = -1;
-    float reg[kSlots];
     float v = 0.0f;
     if (have) {
-      r = lv_step<W>(G, tv, uid, up, cur, D, v, vm, slot, reg, c);
+      r = lv_step<W>(G, tv, uid, up, cur, D, v, vm, slot, c);
       if (r == kLvDone) {
         lb.value[seed] = v;
         have = false;
@@ -306,8 +314,6 @@ k_level_expand(const GameParams G, const TableView tv, const DealRec* __restrict
           for (int q = 0; q < k; ++q) lb.child[cb + q] = kSeedInvalid;
           lb.value[seed] = 0.0f;
         } else {
-          float strat[kSlots];
-          node_strategy(reg, vm, strat);
           const uint4* src = reinterpret_cast<const uint4*>(&cur);
           uint4* dst = reinterpret_cast<uint4*>(lb.nodes + j);
 #pragma unroll
@@ -316,11 +322,7 @@ k_level_expand(const GameParams G, const TableView tv, const DealRec* __restrict
           uint32_t o = cb;
 #pragma unroll
           for (int a = 0; a < kSlots; ++a)
-            if ((vm >> a) & 1) {
-              lb.child[o] = (j << 3) | (uint32_t)a;
-              lb.cstrat[o] = strat[a];
-              ++o;
-            }
+            if ((vm >> a) & 1) lb.child[o++] = (j << 3) | (uint32_t)a;
         }
         have = false;
       }
@@ -377,7 +379,12 @@ k_level_dfs(const GameParams G, const TableView tv, const DealRec* __restrict__ 
             seed = i;
             const DealRec* D = deals;
             EsState st;
-            lv_seed_state(G, lb, deals, seed, w, batch, up, st, D);
+            if (seed < (uint32_t)batch) {
+              lv_root_state(G, deals, seed, st, D);
+              trav++;
+            } else {
+              lv_child_state(G, lb, deals, w, up, st, D);
+            }
             Ln.cur = st;
             Ln.deal = D;
             Ln.t = st.aux;
@@ -385,7 +392,6 @@ k_level_dfs(const GameParams G, const TableView tv, const DealRec* __restrict__ 
             Ln.sp = 0;
             Ln.value = 0.0f;
             Ln.ret = false;
-            if (seed < (uint32_t)batch) trav++;
             have = true;
           }
         }
@@ -407,10 +413,11 @@ template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 k_level_back(const GameParams G, const TableView tv, const Sched* __restrict__ sched, int batch, float rscale,
              const LevelBufs lb, int L, Counters* __restrict__ counters) {
+  const uint32_t n = lb.ctl->node_count[L];
+  if (n == 0) return;
   __shared__ LevelBase s_base;
   if (threadIdx.x == 0) s_base = level_base(lb, L, batch);
   __syncthreads();
-  const uint32_t n = lb.ctl->node_count[L];
   const uint32_t nb = s_base.node;
   const uint32_t uid = update_id(sched, G.N);
   unsigned upd = 0;
@@ -419,28 +426,24 @@ k_level_back(const GameParams G, const TableView tv, const Sched* __restrict__ s
     const uint32_t vm = m.w;
     if (!vm) continue;
     const unsigned long long slot = m.x;
-    mark_deltas(tv, slot);
-    float vh = 0.0f;
+    // independent of each other: the claim, the row's regrets, the children's values
+    claim_row(tv, slot, uid);
+    float reg[kSlots], strat[kSlots], v[kSlots];
+    load_regrets(tv, (long long)slot, reg);
     uint32_t o = m.z;
 #pragma unroll
-    for (int a = 0; a < kSlots; ++a)
-      if ((vm >> a) & 1) {
-        const float v = __ldcg(lb.value + o);
-        const float s = __ldcg(lb.cstrat + o);
-        ++o;
-        atomicAdd(row_da(tv, slot) + a, (unsigned long long)fix_r(v, rscale));
-        vh = __fadd_rn(vh, __fmul_rn(s, v));
-      }
-    const long long fv = fix_r(vh, rscale);
-    atomicAdd(row_cnt(tv, slot), 1ull << 32);
-    if (touch_row(tv, slot, uid, vm)) {
-      atomicAdd(row_su(tv, slot), (unsigned long long)fv);
-    } else {
-      long long dr[kSlots];
+    for (int a = 0; a < kSlots; ++a) v[a] = ((vm >> a) & 1) ? __ldcg(lb.value + o++) : 0.0f;
+    node_strategy(reg, vm, strat);
+    float vh = 0.0f;
 #pragma unroll
-      for (int b = 0; b < kSlots; ++b) dr[b] = -fv;
-      add_direct(tv, slot, vm, dr, nullptr);
-    }
+    for (int a = 0; a < kSlots; ++a)
+      if ((vm >> a) & 1) vh = __fadd_rn(vh, __fmul_rn(strat[a], v[a]));
+    const long long fv = fix_r(vh, rscale);
+    mark_deltas(tv, slot);
+#pragma unroll
+    for (int a = 0; a < kSlots; ++a)
+      if ((vm >> a) & 1) atomicAdd(row_da(tv, slot) + a, (unsigned long long)(fix_r(v[a], rscale) - fv));
+    atomicAdd(row_cnt(tv, slot), 1ull << 32);
     upd++;
     lb.value[m.y] = vh;
   }

@@ -63,12 +63,13 @@ __device__ __forceinline__ void warp_add_counters(Counters* c, unsigned t, unsig
   u = __reduce_add_sync(m, u);
   x = __reduce_add_sync(m, x);
   e = __reduce_add_sync(m, e);
+  // only non-zero sums are added: a launch over an empty level adds nothing
   if ((threadIdx.x & 31) == (__ffs(m) - 1)) {
-    atomicAdd(&c->traversals, (unsigned long long)t);
-    atomicAdd(&c->visits, (unsigned long long)v);
-    atomicAdd(&c->updates, (unsigned long long)u);
-    atomicAdd(&c->terminals, (unsigned long long)x);
-    atomicAdd(&c->evals, (unsigned long long)e);
+    if (t) atomicAdd(&c->traversals, (unsigned long long)t);
+    if (v) atomicAdd(&c->visits, (unsigned long long)v);
+    if (u) atomicAdd(&c->updates, (unsigned long long)u);
+    if (x) atomicAdd(&c->terminals, (unsigned long long)x);
+    if (e) atomicAdd(&c->evals, (unsigned long long)e);
   }
 }
 
@@ -533,7 +534,7 @@ k_traverse_ref(const GameParams G, const TableView tv, const DealRec* __restrict
     const int s = (int)(sv & 0xFF);
     const uint32_t vm = sv >> 8;
     const long long dsamp = fix_r(__fsub_rn(__fdiv_rn(u, s_rec_q[i][tid]), u), rscale);
-    if (touch_row(tv, slot, uid, vm)) {
+    if (touch_row(tv, slot, uid, vm, true)) {
       atomicAdd(row_cnt(tv, slot), (1ull << 32) | 1ull);
       atomicAdd(row_su(tv, slot), (unsigned long long)fu);
       mark_deltas(tv, slot);
