@@ -78,18 +78,18 @@ def make_config(L, workload: str, rank: int = 0):
 
 def apply_roofline(s0, s1, launches: int, peak: float) -> dict:
     """The apply kernel's share of a step against the HBM roofline: per touched
-    row its first 128-byte line read and written and its 4-byte list entry read
-    (260 B), plus the second line read and written (256 B) for the rows that
-    hold the updating player's accumulators; rows counted on the device for the
-    last player-update."""
+    row both 128-byte lines read, the first written and its 4-byte list entry
+    read (388 B), plus the second line written (128 B) for the rows that hold
+    accumulators; rows counted on the device for the last player-update."""
     ms = (s1.apply_ms - s0.apply_ms) / max(1, launches)
     rows = int(s1.touched_last)
     wide = int(getattr(s1, "wide_rows_last", 0))
-    nbytes = rows * 260.0 + wide * 256.0
+    nbytes = rows * 388.0 + wide * 128.0
     gbs = nbytes / (ms / 1e3) / 1e9 if ms > 0 else None
     return {"kernel": "k_apply", "kernel_ms_per_launch": ms, "touched_rows_last_update": rows,
             "wide_rows_last_update": wide, "bytes_per_launch": nbytes,
-            "bytes_per_row": "260 (first line + list entry) + 256 for rows with regret accumulators",
+            "bytes_per_row": "388 (both lines read, first written, list entry) + 128 (second line written) for "
+                             "rows with accumulators",
             "achieved": gbs, "unit": "GB/s", "frac": gbs / peak if gbs else None}
 
 

@@ -59,19 +59,16 @@ constexpr int kRefBlock = 128;
 __device__ __forceinline__ void apply_rows(const GameParams& G, const TableView& tv, const Sched* sched, double rinv,
                                            unsigned group, unsigned ngroups, bool leader) {
   const uint32_t uid = update_id(sched, G.N);
-  const unsigned n_narrow = tv.n_touched[uid & 1];
-  const unsigned n = n_narrow + tv.n_touched[2 + (uid & 1)];
+  const unsigned n = tv.n_touched[uid & 1];
   const double w = G.lcfr ? (double)(float)sched->iteration : 1.0;
   const double s32 = 2.3283064365386962890625e-10;  // 2^-32
   const int a = threadIdx.x & 7;
   const unsigned gmask = 0xFFu << (threadIdx.x & 24);
-  unsigned wide_rows = 0;  // rows whose second line was folded too (counted by lane 0 of each group)
+  unsigned wide_rows = 0;  // rows whose second line was written back (counted by lane 0 of each group)
   for (unsigned i = group; i < n; i += ngroups) {
-    // the narrow list's rows were first touched by sampled opponents and hold
-    // no regret accumulators unless a flag says so (a shared key); the wide
-    // list's rows always do, so both their lines are read at once
-    const bool listed_wide = i >= n_narrow;
-    const unsigned long long slot = listed_wide ? tv.touched_wide[i - n_narrow] : tv.touched[i];
+    const unsigned long long slot = tv.touched[i];
+    // every field of both lines is loaded at once: a row's accumulators are
+    // zero unless its flags say they were written, so no load waits on another
     const uint32_t m = (uint32_t)(*row_tag(tv, slot) & 0xFF);
     const unsigned long long cnt = *row_cnt(tv, slot);
     const long long canon = (long long)(cnt & 0xFFFFFFFFull);
@@ -83,11 +80,8 @@ __device__ __forceinline__ void apply_rows(const GameParams& G, const TableView&
     long long* dsp = reinterpret_cast<long long*>(row_ds(tv, slot));
     const float r_a = regp[a];
     const float s_a = ssp[a];
-    long long da_a = 0;
-    if (listed_wide) da_a = dap[a];
-    const bool has_da = listed_wide || (flags & kFlagDa);
-    if (!listed_wide && (flags & kFlagDa)) da_a = dap[a];
-    const long long ds_a = (flags & kFlagDs) ? dsp[a] : 0ll;
+    const long long da_a = dap[a];
+    const long long ds_a = dsp[a];
     // strategy of the canonical mask from the snapshot regrets (node_strategy)
     float sum_r = 0.0f;
 #pragma unroll
@@ -104,23 +98,22 @@ __device__ __forceinline__ void apply_rows(const GameParams& G, const TableView&
     if (G.cfr_plus) r = (r < 0.0f) ? 0.0f : r;
     regp[a] = r;
     ssp[a] = __fadd_rn(s_a, __double2float_rn(__dmul_rn(__dmul_rn((double)dsv, s32), w)));
-    if (has_da) dap[a] = 0;
+    if (flags & kFlagDa) dap[a] = 0;
     if (flags & kFlagDs) dsp[a] = 0;
     if (a == 0) {
       *row_visits(tv, slot) += cnt >> 32;
       *row_cnt(tv, slot) = 0;
       *row_su(tv, slot) = 0;
       *row_flags(tv, slot) = 0;
-      wide_rows += (has_da || (flags & kFlagDs)) ? 1u : 0u;
+      wide_rows += (flags & (kFlagDa | kFlagDs)) ? 1u : 0u;
     }
   }
   wide_rows = __reduce_add_sync(0xFFFFFFFFu, wide_rows);
-  if ((threadIdx.x & 31) == 0 && wide_rows) atomicAdd(tv.n_touched + 4 + (uid & 1), wide_rows);
+  if ((threadIdx.x & 31) == 0 && wide_rows) atomicAdd(tv.n_touched + 2 + (uid & 1), wide_rows);
   if (leader) {
     const uint32_t next = (uid + 1) & 1;
     tv.n_touched[next] = 0;
     tv.n_touched[2 + next] = 0;
-    tv.n_touched[4 + next] = 0;
   }
 }
 
@@ -1061,14 +1054,13 @@ int mccfr_create(const mccfr_config* cfg, mccfr_handle** out) {
   // Table rows, the touched list and small counters in one allocation.
   h->cap = 1ull << cfg->table_log2;
   const unsigned long long C = h->cap;
-  const size_t bytes_rows = C * kRowBytes, bytes_touch = C * 8, bytes_misc = 256;  // two touched lists
+  const size_t bytes_rows = C * kRowBytes, bytes_touch = C * 4, bytes_misc = 256;
   h->block_bytes = bytes_rows + bytes_touch + bytes_misc;
   CKC(cudaMalloc(&h->d_block, bytes_rows + bytes_touch + bytes_misc));
   CKC(cudaMemset(h->d_block, 0, bytes_rows + bytes_touch + bytes_misc));
   char* base = static_cast<char*>(h->d_block);
   h->tv.rows = reinterpret_cast<unsigned char*>(base);
   h->tv.touched = reinterpret_cast<unsigned int*>(base + bytes_rows);
-  h->tv.touched_wide = reinterpret_cast<unsigned int*>(base + bytes_rows + C * 4);
   char* misc = base + bytes_rows + bytes_touch;
   h->tv.n_touched = reinterpret_cast<unsigned int*>(misc);
   h->tv.err = reinterpret_cast<int*>(misc + 64);
@@ -1215,12 +1207,12 @@ int mccfr_step(mccfr_handle* h, long long iteration, int player, int batch, mccf
     h->traverse_ms += t1;
     h->apply_ms += t2;
     h->launches++;
-    unsigned nt[6] = {0, 0, 0, 0, 0, 0};
+    unsigned nt[4] = {0, 0, 0, 0};
     cudaMemcpy(nt, h->tv.n_touched, sizeof(nt), cudaMemcpyDeviceToHost);
     // the apply kernel resets the other parity's counters, not this one's
     const uint32_t par = (uint32_t)((iteration - 1) * h->cfg.num_players + player) & 1;
-    h->touched_last = (long long)nt[par] + nt[2 + par];
-    h->wide_last = nt[4 + par];
+    h->touched_last = nt[par];
+    h->wide_last = nt[2 + par];
     rc = check_device_error(h);
   }
   if (rc == MCCFR_OK && trace) {
@@ -1262,11 +1254,11 @@ int mccfr_train(mccfr_handle* h, long long iters, int batch, int verbose, const 
       if (i + 1 == iters) {
         // rows touched by this iteration's last player-update (its parity's counter
         // is reset only by the next update's apply)
-        unsigned nt[6] = {0, 0, 0, 0, 0, 0};
+        unsigned nt[4] = {0, 0, 0, 0};
         CK(cudaMemcpy(nt, h->tv.n_touched, sizeof(nt), cudaMemcpyDeviceToHost));
         const uint32_t par = (uint32_t)((base + i) * np + np - 1) & 1;
-        h->touched_last = (long long)nt[par] + nt[2 + par];
-        h->wide_last = nt[4 + par];
+        h->touched_last = nt[par];
+        h->wide_last = nt[2 + par];
       }
     }
     h->launches += h->cfg.num_players;

@@ -17,8 +17,9 @@
 //   128  da[8]  i64   per-action regret deltas, 2^-rb units
 //   192  ds[8]  i64   strategy weights of non-canonical visits, 2^-32 units
 // tag/cnt/su/da/ds/flags are per-update accumulators, zeroed by the apply
-// kernel, which reads and writes the second line only when a flag says it holds
-// values.
+// kernel.  The second line is zero unless a flag says it holds values (every
+// writer sets the flag), so the apply kernel reads both lines at once and
+// writes the second back only for flagged rows.
 #pragma once
 #include <cstdint>
 
@@ -31,10 +32,9 @@ constexpr unsigned kFlagDs = 1u, kFlagDa = 2u;
 
 struct TableView {
   unsigned char* rows;       // [cap][256]
-  unsigned int* touched;     // [cap] rows first touched by a sampled opponent (first line only, as a rule)
-  unsigned int* touched_wide;  // [cap] rows first touched by an updating-player node (both lines)
-  // [6], each pair by update-id parity: entries of `touched`, of `touched_wide`,
-  // and rows whose second line the apply kernel folded
+  unsigned int* touched;     // [cap] rows touched by the update, in order of first touch
+  // [4], each pair by update-id parity: entries of `touched`, and rows whose
+  // second line the apply kernel folded
   unsigned int* n_touched;
   unsigned long long mask;   // cap - 1
   int log2cap;
@@ -139,28 +139,22 @@ __device__ __forceinline__ long long table_insert(const TableView& tv, unsigned 
   return -1;
 }
 
-__device__ __forceinline__ void list_row(const TableView& tv, unsigned long long slot, uint32_t uid, bool wide) {
-  if (wide) {
-    const unsigned int i = atomicAdd(tv.n_touched + 2 + (uid & 1), 1u);
-    tv.touched_wide[i] = (unsigned int)slot;
-  } else {
-    const unsigned int i = atomicAdd(tv.n_touched + (uid & 1), 1u);
-    tv.touched[i] = (unsigned int)slot;
-  }
+__device__ __forceinline__ void list_row(const TableView& tv, unsigned long long slot, uint32_t uid) {
+  const unsigned int i = atomicAdd(tv.n_touched + (uid & 1), 1u);
+  tv.touched[i] = (unsigned int)slot;
 }
 
 // Marks the row as touched by update `uid`; returns whether `vm` is the
-// update's canonical mask for that row (the first visitor sets it).  The row
-// goes to the wide list when the first visitor will write regret accumulators.
+// update's canonical mask for that row (the first visitor sets it).
 __device__ __forceinline__ bool touch_row(const TableView& tv, unsigned long long slot, uint32_t uid,
-                                          uint32_t vm, bool wide = false) {
+                                          uint32_t vm) {
   const unsigned long long want = ((unsigned long long)(uid + 1) << 8) | vm;
   unsigned long long* tag = row_tag(tv, slot);
   unsigned long long old = __ldcg(tag);
   if ((old >> 8) != (unsigned long long)(uid + 1)) {
     const unsigned long long r = atomicCAS(tag, old, want);
     if (r == old) {
-      list_row(tv, slot, uid, wide);
+      list_row(tv, slot, uid);
       return true;
     }
     old = r;
@@ -175,7 +169,7 @@ __device__ __forceinline__ bool touch_row(const TableView& tv, unsigned long lon
 // leaves a tag of this update (claimed or not) as it is.
 __device__ __forceinline__ void claim_row(const TableView& tv, unsigned long long slot, uint32_t uid) {
   const unsigned long long old = atomicMax(row_tag(tv, slot), (unsigned long long)(uid + 1) << 8);
-  if ((old >> 8) < (unsigned long long)(uid + 1)) list_row(tv, slot, uid, true);
+  if ((old >> 8) < (unsigned long long)(uid + 1)) list_row(tv, slot, uid);
 }
 
 // Marks the row's regret accumulators (second line) as holding values in this

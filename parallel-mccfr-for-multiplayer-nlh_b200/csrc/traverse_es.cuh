@@ -319,7 +319,7 @@ __device__ __forceinline__ int es_step(const GameParams& G, const TableView& tv,
       const float vh = F.vh;
       const long long fv = fix_r(vh, rscale);
       atomicAdd(row_cnt(tv, F.slot), 1ull << 32);
-      if (touch_row(tv, F.slot, uid, F.vm, true)) {
+      if (touch_row(tv, F.slot, uid, F.vm)) {
         atomicAdd(row_su(tv, F.slot), (unsigned long long)fv);
       } else {
         long long dr[kSlots];

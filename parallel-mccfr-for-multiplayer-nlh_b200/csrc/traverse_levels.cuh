@@ -92,6 +92,30 @@ __device__ __forceinline__ LevelBase level_base(const LevelBufs& lb, int L, int 
 
 enum { kLvGoOn = 0, kLvDone = 1, kLvUp = 2 };
 
+// Side-pot showdown payoff of the updating player (side_pot_payoff), kept out
+// of line so that the loop the lanes share stays small in the instruction
+// cache; the invested chips come packed two per word, by value.
+__device__ __noinline__ float lv_showdown(int N, int up, uint32_t folded, uint32_t inv01, uint32_t inv23,
+                                          uint32_t inv45, const DealRec* D) {
+  const uint32_t w[3] = {inv01, inv23, inv45};
+  return side_pot_payoff(
+      N, up, folded, [&](int q) { return (int)((w[q >> 1] >> (16 * (q & 1))) & 0xFFFF); },
+      [&](int q) { return (uint32_t)__ldg(D->rank + q); });
+}
+
+// A sampled opponent's visit whose mask is not the row's canonical one: its
+// strategy weights go to the accumulators directly.
+__device__ __forceinline__ void lv_off_canonical(const TableView& tv, unsigned long long slot, uint32_t vm,
+                                                 const float* reg) {
+  atomicAdd(row_cnt(tv, slot), 1ull << 32);
+  float strat[kSlots];
+  node_strategy(reg, vm, strat);
+  long long dw[kSlots];
+#pragma unroll
+  for (int a = 0; a < kSlots; ++a) dw[a] = fix_s(strat[a]);
+  add_direct(tv, slot, vm, nullptr, dw);
+}
+
 // One step of a seed's walk (the descend branch of es_step): the cheap steps
 // (depth cut, fold win, street change, showdown), then at most one decision
 // node.  An opponent's node is done here; at an updating-player node the walk
@@ -134,8 +158,9 @@ __device__ __forceinline__ int lv_step(const GameParams& G, const TableView& tv,
         continue;
       }
     }
-    value = side_pot_payoff(
-        N, up, cur.folded, [&](int q) { return pget(cur.inv, q); }, [&](int q) { return (uint32_t)__ldg(D->rank + q); });
+    value = lv_showdown(N, up, cur.folded, (uint32_t)cur.inv[0] | ((uint32_t)cur.inv[1] << 16),
+                        (uint32_t)cur.inv[2] | ((uint32_t)cur.inv[3] << 16),
+                        (uint32_t)cur.inv[4] | ((uint32_t)cur.inv[5] << 16), D);
     cnt.terminals++;
     return kLvDone;
   }
@@ -169,13 +194,7 @@ __device__ __forceinline__ int lv_step(const GameParams& G, const TableView& tv,
     if (touch_row(tv, (unsigned long long)slot, uid, vm)) {
       atomicAdd(row_cnt(tv, slot), (1ull << 32) | 1ull);
     } else {
-      atomicAdd(row_cnt(tv, slot), 1ull << 32);
-      float strat[kSlots];
-      node_strategy(reg, vm, strat);
-      long long dw[kSlots];
-#pragma unroll
-      for (int a = 0; a < kSlots; ++a) dw[a] = fix_s(strat[a]);
-      add_direct(tv, slot, vm, nullptr, dw);
+      lv_off_canonical(tv, (unsigned long long)slot, vm, reg);
     }
   }
   es_apply(G, cur, player, s);
@@ -209,8 +228,10 @@ __device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) { return *(vo
 
 // ROOT: level 0, whose seeds are the traversals' roots (built from the deals);
 // deeper levels load their parent's state instead.
+// Eight blocks of 128 threads per SM (64 registers): the walk waits on
+// dependent table reads, so resident warps matter more than a few spills.
 template <int BLOCK, int W, bool ROOT>
-__global__ void __launch_bounds__(BLOCK)
+__global__ void __launch_bounds__(BLOCK, 8)
 k_level_expand(const GameParams G, const TableView tv, const DealRec* __restrict__ deals,
                const Sched* __restrict__ sched, int batch, const LevelBufs lb, int L,
                Counters* __restrict__ counters) {

@@ -534,7 +534,7 @@ k_traverse_ref(const GameParams G, const TableView tv, const DealRec* __restrict
     const int s = (int)(sv & 0xFF);
     const uint32_t vm = sv >> 8;
     const long long dsamp = fix_r(__fsub_rn(__fdiv_rn(u, s_rec_q[i][tid]), u), rscale);
-    if (touch_row(tv, slot, uid, vm, true)) {
+    if (touch_row(tv, slot, uid, vm)) {
       atomicAdd(row_cnt(tv, slot), (1ull << 32) | 1ull);
       atomicAdd(row_su(tv, slot), (unsigned long long)fu);
       mark_deltas(tv, slot);

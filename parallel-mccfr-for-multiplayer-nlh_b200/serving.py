@@ -105,9 +105,9 @@ def request_config(req: Request) -> L.Config:
 
 
 def table_bytes(req: Request) -> int:
-    """Device bytes of a request's table: 256-byte rows and two 4-byte touched-list
-    entries per row, plus its small buffers."""
-    return (1 << req.table_log2) * (256 + 8) + (1 << 20)
+    """Device bytes of a request's table: 256-byte rows and a 4-byte touched-list
+    entry per row, plus its small buffers."""
+    return (1 << req.table_log2) * (256 + 4) + (1 << 20)
 
 
 @dataclass
@@ -204,7 +204,7 @@ class ReSolveServer:
         return int(torch.cuda.mem_get_info()[0])
 
     def pooled_bytes(self) -> int:
-        return sum((1 << log2) * (256 + 8) + (1 << 20) for log2, ts in self.pool.items() for _ in ts)
+        return sum((1 << log2) * (256 + 4) + (1 << 20) for log2, ts in self.pool.items() for _ in ts)
 
     def _evict(self, need: int, held: int) -> None:
         """Frees pooled tables of other capacities until `need` more bytes fit."""
