@@ -78,18 +78,19 @@ def make_config(L, workload: str, rank: int = 0):
 
 def apply_roofline(s0, s1, launches: int, peak: float) -> dict:
     """The apply kernel's share of a step against the HBM roofline: per touched
-    row both 128-byte lines read, the first written and its 4-byte list entry
-    read (388 B), plus the second line written (128 B) for the rows that hold
-    accumulators; rows counted on the device for the last player-update."""
+    row the 256-byte record read, its first 128-byte line and last sector written
+    and its 4-byte list entry read (420 B), plus the regret and strategy-weight
+    accumulators written back (96 B) for the rows that hold them; rows counted
+    on the device for the last player-update."""
     ms = (s1.apply_ms - s0.apply_ms) / max(1, launches)
     rows = int(s1.touched_last)
     wide = int(getattr(s1, "wide_rows_last", 0))
-    nbytes = rows * 388.0 + wide * 128.0
+    nbytes = rows * 420.0 + wide * 96.0
     gbs = nbytes / (ms / 1e3) / 1e9 if ms > 0 else None
     return {"kernel": "k_apply", "kernel_ms_per_launch": ms, "touched_rows_last_update": rows,
             "wide_rows_last_update": wide, "bytes_per_launch": nbytes,
-            "bytes_per_row": "388 (both lines read, first written, list entry) + 128 (second line written) for "
-                             "rows with accumulators",
+            "bytes_per_row": "420 (record read, first line and flags sector written, list entry) + 96 "
+                             "(accumulators written back) for rows that hold them",
             "achieved": gbs, "unit": "GB/s", "frac": gbs / peak if gbs else None}
 
 
@@ -455,6 +456,64 @@ def multitable(m, L, table, iters=2) -> dict:
                         "LogNormal(14,1)/16, seed 2; wall clock over iterations 2-3 of fresh tables, both forms"}
 
 
+def batched_small_tables(m, L, table, n_tables=64, batch=4096, iters=3) -> dict:
+    """The regime a multi-table kernel is for: 64 independent 6-max 100BB tables
+    (2^20-row tables, 20-bit keys, seeds 100..163) of 4,096 traversals per
+    player-update each.  Plain: every table's iteration on its own (one graph
+    replay each, the level-synchronous kernels), one table after another;
+    batched: all 64 in one persistent traversal launch per phase.  Both over the
+    same iterations of fresh tables, wall clock; rows are bit-identical between
+    the two (tests/test_gpu_batched.py)."""
+    import torch
+
+    def make():
+        ts = []
+        for i in range(n_tables):
+            c = L.preset(L.PRESET_6MAX_100BB)
+            c.table_log2, c.key_bits, c.seed = 20, 20, 100 + i
+            t = m.GPUCFRTrainer(config=c)
+            t.set_hand_table(table)
+            ts.append(t)
+        return ts
+
+    plain = make()
+    for t in plain:
+        t.train(1, batch, verbose=False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(iters):
+        for t in plain:
+            t.train(1, batch, verbose=False)
+    torch.cuda.synchronize()
+    plain_s = time.perf_counter() - t0
+    for t in plain:
+        t.close()
+    scratch = make()
+    sb = m.Batch(scratch, [batch] * n_tables)
+    best = sb.autotune(max_candidates=16)
+    sb.close()
+    for t in scratch:
+        t.close()
+    batched = make()
+    b = m.Batch(batched, [batch] * n_tables)
+    b.set_tuning(**best)
+    b.train(1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.train(iters)
+    torch.cuda.synchronize()
+    batched_s = time.perf_counter() - t0
+    b.close()
+    for t in batched:
+        t.close()
+    trav = iters * n_tables * batch * 6
+    return {"tables": n_tables, "traversals_per_update": batch, "iterations": iters,
+            "plain_traversals_per_s": trav / plain_s, "batched_traversals_per_s": trav / batched_s,
+            "speedup": plain_s / batched_s, "tuning": best,
+            "workload": "64 tables of 6-max 100BB, 4,096 traversals per player-update each, iterations 2-4 of "
+                        "fresh tables, wall clock, both forms"}
+
+
 def serving_sweep(m, L, table, rates=(10, 30, 100, 300, 1000), n_requests=48) -> dict:
     """Re-solve serving at several Poisson arrival rates: p50/p99 latency (arrival
     to strategy on the host) and solves/s, continuous batching on one B200."""
@@ -601,6 +660,59 @@ def c4_showdown(m, L, table, total=1 << 28, chunk=1 << 24, deals6=1 << 24) -> di
                         "table). 6-seat: 2^24 deals of training's 6-player deal (iteration 1, player 0), "
                         "k_showdown_masks (board walked once, 2 gathers per seat, winner/split mask per deal); "
                         "both bit-exact with the oracle in tests/test_gpu_showdown.py"}
+
+
+def reference_gpu(m, L, table, iters: int = 20) -> dict:
+    """The reference's own GPU trainer (poker_cuda/src/cfr_gpu.cu compiled
+    unchanged for sm_100a, oracle/_ref/libref_gpu.so) on this box, in a child
+    process, beside this trainer's reference rule on the same game: the
+    reference's benchmark configurations (main.cpp:380-398; players and blinds of
+    scripts/carc_train.sh:75-80), `iters` iterations from a fresh trainer.  Its
+    own figure is the rate its training loop prints (cfr_gpu.cu:1368-1377,
+    after allocation and graph capture); ours is CUDA-event time of the same
+    iterations after the same start."""
+    import re
+    import tempfile
+
+    import torch
+
+    lib_path = ROOT / "oracle" / "_ref" / "libref_gpu.so"
+    if not lib_path.exists():
+        return {"unavailable": "the reference's GPU trainer was not built (its sources were absent at build time)"}
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        table_file = Path(d) / "handranks.dat"
+        table.tofile(table_file)
+        for players, batch in ((6, 262144), (6, 65536), (2, 65536)):
+            r = subprocess.run([sys.executable, str(ROOT / "oracle" / "ref_gpu_run.py"), "time", str(players),
+                                str(iters), str(batch), str(table_file)], capture_output=True, text=True, timeout=900)
+            line = {"returncode": r.returncode}
+            mdone = re.search(r"\(([\d.]+)M hands/sec\)", r.stdout)
+            if mdone:
+                line["reference_loop_traversals_per_s"] = float(mdone.group(1)) * 1e6
+            for ln in r.stdout.splitlines():
+                if ln.startswith("{"):
+                    line["reference_benchmark_mode_traversals_per_s"] = json.loads(ln)["traversals_per_s"]
+            cfg = L.preset(L.PRESET_REF8)
+            cfg.num_players = players
+            t = m.GPUCFRTrainer(config=cfg)
+            t.set_hand_table(table)
+            t.train(1, batch, verbose=False)  # graph capture, as the reference's loop figure excludes it
+            st = torch.cuda.ExternalStream(t.stream_ptr())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            t.train(iters - 1, batch, verbose=False)
+            e1.record(st)
+            e1.synchronize()
+            t.close()
+            ours = (iters - 1) * batch * players / (e0.elapsed_time(e1) / 1e3)
+            line["ours_traversals_per_s"] = ours
+            if "reference_loop_traversals_per_s" in line:
+                line["ours_over_reference"] = ours / line["reference_loop_traversals_per_s"]
+            out[f"{players}p_batch{batch}"] = line
+    out["workload"] = (f"the reference's game: stack 1000, blinds 10/20, 8 action slots, 64/128 buckets, its update "
+                       f"rule (outcome sampling at the updating player), {iters} iterations of a fresh trainer")
+    return out
 
 
 def hu_full_exploitability(m, L, table, iters: int, stride: int) -> dict:
@@ -822,9 +934,11 @@ def main():
 
         extra("batched_same_table", lambda: batched_same_table(m, L, table, args, value))
         extra("c3_multitable", lambda: multitable(m, L, table))
+        extra("batched_small_tables", lambda: batched_small_tables(m, L, table))
         extra("resolve_serving", lambda: serving_sweep(m, L, table))
         extra("hu_subgame_exploitability", lambda: hu_subgame_exploitability(m, L, table))
         extra("c4_showdown", lambda: c4_showdown(m, L, table))
+        extra("reference_gpu", lambda: reference_gpu(m, L, table))
         for wl in ("ref8-6max", "6max-100bb-refrule"):
             if wl != args.workload:
                 extra(wl, lambda wl=wl: refrule_rate(wl))

@@ -157,9 +157,8 @@ typedef struct mccfr_stats {
   double last_traverse_ms;
   double last_apply_ms;
   int32_t device_error;      /* sticky kernel error bits */
-  /* rows of the last player-update whose second 128-byte line (regret
-     accumulators, or strategy weights of visits off the canonical mask) held
-     values and was written back as well as the first */
+  /* rows of the last player-update whose regret accumulators (or strategy
+     weights of visits off the canonical mask) held values and were written back */
   int32_t wide_rows_last;
   int32_t reserved[6];
 } mccfr_stats;

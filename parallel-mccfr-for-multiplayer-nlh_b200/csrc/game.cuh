@@ -194,7 +194,8 @@ __device__ __forceinline__ int sample_action(const GameParams& G, const float* r
   for (int a = 0; a < kSlots; ++a) {
     sig[a] = 0.0f;
     if ((vm >> a) & 1) {
-      sig[a] = bf16_round(__fdiv_rn(fmaxf(0.0f, reg[a]), sum));
+      // a clamped (non-positive) regret gives +0 exactly: no division needed
+      if (reg[a] > 0.0f) sig[a] = bf16_round(__fdiv_rn(reg[a], sum));
       total = __fadd_rn(total, sig[a]);
     }
   }
@@ -220,12 +221,19 @@ __device__ __forceinline__ void node_strategy(const float* reg, uint32_t vm, flo
     if ((vm >> a) & 1) sum_r = __fadd_rn(sum_r, fmaxf(0.0f, reg[a]));
   if (sum_r > 1e-7f) {
 #pragma unroll
-    for (int a = 0; a < kSlots; ++a) strat[a] = ((vm >> a) & 1) ? __fdiv_rn(fmaxf(0.0f, reg[a]), sum_r) : 0.0f;
+    for (int a = 0; a < kSlots; ++a) strat[a] = ((vm >> a) & 1) && reg[a] > 0.0f ? __fdiv_rn(reg[a], sum_r) : 0.0f;
   } else {
     const float uni = __fdiv_rn(1.0f, (float)__popc(vm));
 #pragma unroll
     for (int a = 0; a < kSlots; ++a) strat[a] = ((vm >> a) & 1) ? uni : 0.0f;
   }
+}
+
+// Seat p + i (0 <= p < N, 0 <= i <= N) around a table of N seats, without a
+// division.
+__host__ __device__ __forceinline__ int seat_after(int p, int i, int N) {
+  const int s = p + i;
+  return s >= N ? s - N : s;
 }
 
 // Per-player fields indexed by a runtime player: selects over the unrolled

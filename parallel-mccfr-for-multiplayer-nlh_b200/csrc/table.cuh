@@ -1,10 +1,9 @@
 // table.cuh — open-addressed info-set table in HBM.
 //
 // Replaces the reference's direct-mapped SoA tables [8 x 2^26] (cfr_gpu.cu:
-// 1106-1136).  Each row is one 256-byte record of two 128-byte lines.  The first
-// line holds everything a visit reads and everything a row touched only by
-// sampled opponents needs folded; the second holds the per-action accumulators
-// of the updating player's nodes:
+// 1106-1136).  Each row is one 256-byte record (two 128-byte lines), so that a
+// visit touches two adjacent sectors and folding a row in reads one contiguous
+// record instead of a dozen scattered ones:
 //     0  key    u64   0 = empty; linear probing from the key's home slot, or row k-1
 //                       for key k when every key is at most the capacity (direct map)
 //     8  tag    u64   ((update id + 1) << 8) | canonical action mask of that update
@@ -12,22 +11,22 @@
 //    24  su     i64   sum of fix(u) (reference rule) or fix(v_h) (external sampling)
 //    32  reg[8] f32   regrets: read by every visit (snapshot within an update)
 //    64  ssum[8] f32  average-strategy sums
-//    96  visits u64   updates received since creation
-//   104  flags  u32   bit 0: ds holds values; bit 1: da holds values
-//   128  da[8]  i64   per-action regret deltas, 2^-rb units
-//   192  ds[8]  i64   strategy weights of non-canonical visits, 2^-32 units
+//    96  da[8]  i64   per-action regret deltas, 2^-rb units
+//   160  ds[8]  i64   strategy weights of non-canonical visits, 2^-32 units
+//   224  visits u64   updates received since creation
+//   232  flags  u32   bit 0: ds holds values; bit 1: da holds values
 // tag/cnt/su/da/ds/flags are per-update accumulators, zeroed by the apply
-// kernel.  The second line is zero unless a flag says it holds values (every
-// writer sets the flag), so the apply kernel reads both lines at once and
-// writes the second back only for flagged rows.
+// kernel.  da and ds are zero unless a flag says they were written (every
+// writer sets its flag), so the apply kernel loads the whole record at once and
+// writes them back only for flagged rows.
 #pragma once
 #include <cstdint>
 
 namespace mccfr {
 
 constexpr int kRowBytes = 256;
-constexpr int kOffKey = 0, kOffTag = 8, kOffCnt = 16, kOffSu = 24, kOffReg = 32, kOffSsum = 64, kOffVisits = 96,
-              kOffFlags = 104, kOffDa = 128, kOffDs = 192;
+constexpr int kOffKey = 0, kOffTag = 8, kOffCnt = 16, kOffSu = 24, kOffReg = 32, kOffSsum = 64, kOffDa = 96,
+              kOffDs = 160, kOffVisits = 224, kOffFlags = 232;
 constexpr unsigned kFlagDs = 1u, kFlagDa = 2u;
 
 struct TableView {
@@ -172,8 +171,8 @@ __device__ __forceinline__ void claim_row(const TableView& tv, unsigned long lon
   if ((old >> 8) < (unsigned long long)(uid + 1)) list_row(tv, slot, uid);
 }
 
-// Marks the row's regret accumulators (second line) as holding values in this
-// update; every writer of da calls it at least once before its first add.
+// Marks the row's regret accumulators as holding values in this update; every
+// writer of da calls it at least once before its first add.
 __device__ __forceinline__ void mark_deltas(const TableView& tv, unsigned long long slot) {
   atomicOr(row_flags(tv, slot), kFlagDa);
 }

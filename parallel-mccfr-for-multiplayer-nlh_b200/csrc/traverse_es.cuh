@@ -80,7 +80,7 @@ __device__ __forceinline__ void es_apply(const GameParams& G, EsState& s, int pl
     s.q = 0;
     s.nq = 0;
     for (int i = 1; i < G.N; ++i) {
-      const int p = (player + i) % G.N;
+      const int p = seat_after(player, i, G.N);
       if (!((s.folded >> p) & 1) && !((s.allin >> p) & 1)) s.q |= (uint32_t)p << (4 * s.nq++);
     }
   }
@@ -147,14 +147,14 @@ __device__ __forceinline__ void es_begin(const GameParams& G, const DealRec* D, 
     L.cur.depth = 0;
     L.cur.q = 0;
     L.cur.nq = 0;
-    for (int i = 1; i <= N; ++i) L.cur.q |= (uint32_t)((dealer + i) % N) << (4 * L.cur.nq++);
+    for (int i = 1; i <= N; ++i) L.cur.q |= (uint32_t)seat_after(dealer, i, N) << (4 * L.cur.nq++);
   } else {
     for (int p = 0; p < kMaxPlayers; ++p) {
       L.cur.bet[p] = 0;
       L.cur.inv[p] = 0;
     }
-    const int sbp = (N == 2) ? dealer : (dealer + 1) % N;
-    const int bbp = (N == 2) ? (dealer + 1) % N : (dealer + 2) % N;
+    const int sbp = (N == 2) ? dealer : seat_after(dealer, 1, N);
+    const int bbp = (N == 2) ? seat_after(dealer, 1, N) : seat_after(seat_after(dealer, 1, N), 1, N);
     const int sba = min(G.sb, G.stack), bba = min(G.bb, G.stack);
     pset(L.cur.bet, sbp, sba);
     pset(L.cur.inv, sbp, sba);
@@ -175,7 +175,7 @@ __device__ __forceinline__ void es_begin(const GameParams& G, const DealRec* D, 
     L.cur.q = 0;
     L.cur.nq = 0;
     for (int i = 0; i < N; ++i) {
-      const int p = (bbp + 1 + i) % N;
+      const int p = seat_after(seat_after(bbp, 1, N), i, N);
       if (!((L.cur.allin >> p) & 1)) L.cur.q |= (uint32_t)p << (4 * L.cur.nq++);
     }
   }
@@ -236,7 +236,7 @@ __device__ __forceinline__ int es_step(const GameParams& G, const TableView& tv,
         cur.q = 0;
         cur.nq = 0;
         for (int i = 1; i <= N; ++i) {
-          const int p = (L.dealer + i) % N;
+          const int p = seat_after(L.dealer, i, N);
           if (!((cur.folded >> p) & 1) && !((cur.allin >> p) & 1)) cur.q |= (uint32_t)p << (4 * cur.nq++);
         }
         if (cur.nq > 0) {

@@ -150,7 +150,7 @@ __device__ __forceinline__ int lv_step(const GameParams& G, const TableView& tv,
       cur.q = 0;
       cur.nq = 0;
       for (int i = 1; i <= N; ++i) {
-        const int p = (D->dealer + i) % N;
+        const int p = seat_after(D->dealer, i, N);
         if (!((cur.folded >> p) & 1) && !((cur.allin >> p) & 1)) cur.q |= (uint32_t)p << (4 * cur.nq++);
       }
       if (cur.nq > 0) {

@@ -387,10 +387,10 @@ k_traverse_ref(const GameParams G, const TableView tv, const DealRec* __restrict
     pot = G.sub_pot;
     cb = 0;
     street = G.sub_street;
-    for (int i = 1; i <= N; ++i) q |= (uint32_t)((dealer + i) % N) << (4 * nq++);
+    for (int i = 1; i <= N; ++i) q |= (uint32_t)seat_after(dealer, i, N) << (4 * nq++);
   } else {
-    const int sbp = (N == 2) ? dealer : (dealer + 1) % N;
-    const int bbp = (N == 2) ? (dealer + 1) % N : (dealer + 2) % N;
+    const int sbp = (N == 2) ? dealer : seat_after(dealer, 1, N);
+    const int bbp = (N == 2) ? seat_after(dealer, 1, N) : seat_after(seat_after(dealer, 1, N), 1, N);
     const int sba = min(G.sb, G.stack), bba = min(G.bb, G.stack);
     s_stack[sbp][tid] = (uint16_t)(G.stack - sba);
     s_bet[sbp][tid] = (uint16_t)sba;
@@ -403,7 +403,7 @@ k_traverse_ref(const GameParams G, const TableView tv, const DealRec* __restrict
     if (G.stack - sba == 0) allin |= 1u << sbp;
     if (G.stack - bba == 0) allin |= 1u << bbp;
     for (int i = 0; i < N; ++i) {
-      const int p = (bbp + 1 + i) % N;
+      const int p = seat_after(seat_after(bbp, 1, N), i, N);
       if (!((allin >> p) & 1)) q |= (uint32_t)p << (4 * nq++);
     }
   }
@@ -438,7 +438,7 @@ k_traverse_ref(const GameParams G, const TableView tv, const DealRec* __restrict
         q = 0;
         nq = 0;
         for (int i = 1; i <= N; ++i) {
-          const int p = (dealer + i) % N;
+          const int p = seat_after(dealer, i, N);
           if (!((folded >> p) & 1) && !((allin >> p) & 1)) q |= (uint32_t)p << (4 * nq++);
         }
         if (nq > 0) {
@@ -518,7 +518,7 @@ k_traverse_ref(const GameParams G, const TableView tv, const DealRec* __restrict
         q = 0;
         nq = 0;
         for (int i = 1; i < N; ++i) {
-          const int p = (player + i) % N;
+          const int p = seat_after(player, i, N);
           if (!((folded >> p) & 1) && !((allin >> p) & 1)) q |= (uint32_t)p << (4 * nq++);
         }
       }

@@ -56,7 +56,7 @@ def test_apply_roofline():
     s1 = SimpleNamespace(apply_ms=11.0, touched_last=1_000_000, wide_rows_last=250_000)
     a = b.apply_roofline(s0, s1, 2, 6000.0)
     assert a["kernel_ms_per_launch"] == 5.0
-    assert a["achieved"] == pytest.approx((1_000_000 * 388 + 250_000 * 128) / 0.005 / 1e9)
+    assert a["achieved"] == pytest.approx((1_000_000 * 420 + 250_000 * 96) / 0.005 / 1e9)
     assert a["frac"] == pytest.approx(a["achieved"] / 6000.0)
 
 
