@@ -116,16 +116,31 @@ __device__ __forceinline__ void lv_off_canonical(const TableView& tv, unsigned l
   add_direct(tv, slot, vm, nullptr, dw);
 }
 
-// One step of a seed's walk (the descend branch of es_step): the cheap steps
-// (depth cut, fold win, street change, showdown), then at most one decision
-// node.  An opponent's node is done here; at an updating-player node the walk
-// stops with the node's mask and row slot (its regrets are read in back).
+// An action waiting to be applied to a lane's state: the seed's own action
+// (picked up from its parent) or an opponent's sampled one.  Applying it at the
+// top of the next step, instead of where it was chosen, leaves one copy of the
+// action code in the loop, run by all lanes that have an action together.
+struct LvPending {
+  int player;  // -1: none
+  int action;
+};
+
+// One step of a seed's walk (the descend branch of es_step): the pending action,
+// the cheap steps (depth cut, fold win, street change, showdown), then at most
+// one decision node.  An opponent's node is done here (its sampled action is
+// left pending); at an updating-player node the walk stops with the node's mask
+// and row slot (its regrets are read in back).
 template <int W>
 __device__ __forceinline__ int lv_step(const GameParams& G, const TableView& tv, uint32_t uid, int up, EsState& cur,
-                                       const DealRec* D, float& value, uint32_t& vm_out, long long& slot_out,
-                                       EsCounts& cnt) {
+                                       const DealRec* D, LvPending& pend, float& value, uint32_t& vm_out,
+                                       long long& slot_out, EsCounts& cnt) {
   const int N = G.N;
   const uint32_t all_players = (1u << N) - 1;
+  if (pend.player >= 0) {
+    es_apply(G, cur, pend.player, pend.action);
+    cur.depth++;
+    pend.player = -1;
+  }
   for (int guard = 0; guard < 4; ++guard) {
     if (cur.depth >= G.max_depth) {
       value = 0.0f;
@@ -197,22 +212,32 @@ __device__ __forceinline__ int lv_step(const GameParams& G, const TableView& tv,
       lv_off_canonical(tv, (unsigned long long)slot, vm, reg);
     }
   }
-  es_apply(G, cur, player, s);
-  cur.depth++;
+  pend.player = player;
+  pend.action = s;
   return kLvGoOn;
 }
 
-// Start state of a seed of a level below the root: the parent node's state
-// after the seed's action.
-__device__ __forceinline__ void lv_child_state(const GameParams& G, const LevelBufs& lb, const DealRec* deals,
-                                               uint32_t w, int up, EsState& cur, const DealRec*& D) {
+// Start of a seed of a level below the root: the parent node's state, with the
+// seed's action left pending.
+__device__ __forceinline__ void lv_child_start(const LevelBufs& lb, const DealRec* deals, uint32_t w, int up,
+                                               EsState& cur, const DealRec*& D, LvPending& pend) {
   const uint32_t node = (w & ~kSeedDeferred) >> 3;
   const uint4* src = reinterpret_cast<const uint4*>(lb.nodes + node);
   uint4* dst = reinterpret_cast<uint4*>(&cur);
 #pragma unroll
   for (int i = 0; i < 4; ++i) dst[i] = __ldcg(src + i);
   D = deals + cur.aux;
-  es_apply(G, cur, up, (int)(w & 7));
+  pend.player = up;
+  pend.action = (int)(w & 7);
+}
+
+// Start state of a seed below the root, its action applied (the depth-first
+// walk of deferred seeds).
+__device__ __forceinline__ void lv_child_state(const GameParams& G, const LevelBufs& lb, const DealRec* deals,
+                                               uint32_t w, int up, EsState& cur, const DealRec*& D) {
+  LvPending pend;
+  lv_child_start(lb, deals, w, up, cur, D, pend);
+  es_apply(G, cur, pend.player, pend.action);
   cur.depth++;
 }
 
@@ -254,6 +279,7 @@ k_level_expand(const GameParams G, const TableView tv, const DealRec* __restrict
   unsigned trav = 0, deferred = 0;
   EsState cur;
   const DealRec* D = deals;
+  LvPending pend{-1, 0};
   uint32_t seed = 0;
   bool have = false, more = true;
   for (;;) {
@@ -288,7 +314,7 @@ k_level_expand(const GameParams G, const TableView tv, const DealRec* __restrict
               lv_root_state(G, deals, seed, cur, D);
               trav++;
             } else {
-              lv_child_state(G, lb, deals, w, up, cur, D);
+              lv_child_start(lb, deals, w, up, cur, D, pend);
             }
             have = true;
           }
@@ -301,7 +327,7 @@ k_level_expand(const GameParams G, const TableView tv, const DealRec* __restrict
     long long slot = -1;
     float v = 0.0f;
     if (have) {
-      r = lv_step<W>(G, tv, uid, up, cur, D, v, vm, slot, c);
+      r = lv_step<W>(G, tv, uid, up, cur, D, pend, v, vm, slot, c);
       if (r == kLvDone) {
         lb.value[seed] = v;
         have = false;
