@@ -187,12 +187,12 @@ def measured_peak() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def profiled_traffic(workload: str) -> dict | None:
-    """DRAM bytes per traversal of the traversal kernel from a committed ncu
-    summary (profiles/traffic.json), if one exists for this workload."""
+def profiled_traffic(workload: str, form: str) -> dict | None:
+    """DRAM bytes of the traversal kernels from a committed ncu summary
+    (profiles/traffic.json, keyed "workload/form"), if one exists."""
     p = ROOT / "profiles" / "traffic.json"
     try:
-        return json.loads(p.read_text()).get(workload)
+        return json.loads(p.read_text()).get(f"{workload}/{form}")
     except Exception:
         return None
 
@@ -858,10 +858,22 @@ def main():
     bytes_per_launch = (40.0 * visits + 96.0 * updates) / launches
     kernel_ms = trav_ms / launches if trav_ms > 0 else None
     achieved = bytes_per_launch / (kernel_ms / 1e3) / 1e9 if kernel_ms else None
-    tr_prof = profiled_traffic(args.workload)
+    level_form = isinstance(levels, dict) and "seeds" in levels
+    nlev = len(levels["seeds"]) if level_form else 0
+    form_name = "levels" if level_form else ("lanes" if cfg.sampling == 1 else "reference")
+    tr_prof = profiled_traffic(args.workload, form_name)
     traffic = None
-    if tr_prof and "dram_bytes_per_traversal" in tr_prof:
+    if tr_prof and "dram_bytes_per_node_visit" in tr_prof:
+        traffic = tr_prof["dram_bytes_per_node_visit"] * (visits / launches)
+    elif tr_prof and "dram_bytes_per_traversal" in tr_prof:
         traffic = tr_prof["dram_bytes_per_traversal"] * (trav / launches)
+    if level_form:
+        kernel_name = "k_level_expand + k_level_dfs + k_level_back (the traversal of one player-update)"
+        # per update: k_deal, nlev expand levels, k_level_dfs, nlev-1 back levels, k_apply, k_advance
+        launches_per_update = 2 * nlev + 3
+    else:
+        kernel_name = "k_traverse_es" if cfg.sampling == 1 else "k_traverse_ref"
+        launches_per_update = 4  # k_deal, the traversal, k_apply, k_advance
 
     out = {
         "metric": metric, "value": value, "unit": "traversals/s", "n_gpus": world, "steps": args.steps,
@@ -870,13 +882,13 @@ def main():
         "config": {**describe(cfg, args.workload, batch), "parallelism": f"replicas{world}"},
         "e2e": {"value": e2e_value, "unit": "traversals/s", "h2d_bytes_per_step": 16,
                 "d2h_bytes_per_step": 44},
-        # per player-update: k_deal, the traversal kernel, k_apply, k_advance
-        "gpu_launches": int(args.steps * cfg.num_players * 4),
+        "gpu_launches": int(args.steps * cfg.num_players * launches_per_update),
         "clocks": clocks.summary(),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "k_traverse_es" if cfg.sampling == 1 else "k_traverse_ref",
+                     "kernel": kernel_name, "form": form_name,
                      "kernel_ms_per_launch": kernel_ms,
+                     "traffic_source": tr_prof.get("source") if tr_prof else None,
                      "algorithmic_bytes": "40*V + 96*U per launch (V node visits, U updating-player updates)",
                      "V_per_traversal": visits / max(1, trav), "U_per_traversal": updates / max(1, trav)},
         # k_apply folds each touched row: both 128-byte lines of its record read and written, plus
