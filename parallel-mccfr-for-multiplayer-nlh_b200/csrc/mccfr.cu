@@ -59,14 +59,17 @@ constexpr int kRefBlock = 128;
 __device__ __forceinline__ void apply_rows(const GameParams& G, const TableView& tv, const Sched* sched, double rinv,
                                            unsigned group, unsigned ngroups, bool leader) {
   const uint32_t uid = update_id(sched, G.N);
-  const unsigned n = tv.n_touched[uid & 1];
+  const size_t per_shard = (tv.mask + 1) / kListShards;
   const double w = G.lcfr ? (double)(float)sched->iteration : 1.0;
   const double s32 = 2.3283064365386962890625e-10;  // 2^-32
   const int a = threadIdx.x & 7;
   const unsigned gmask = 0xFFu << (threadIdx.x & 24);
   unsigned wide_rows = 0;  // rows whose second line was written back (counted by lane 0 of each group)
+  for (int sh = 0; sh < kListShards; ++sh) {
+  const unsigned n = *list_count(tv, uid & 1, sh);
+  const unsigned* list = tv.touched + (size_t)sh * per_shard;
   for (unsigned i = group; i < n; i += ngroups) {
-    const unsigned long long slot = tv.touched[i];
+    const unsigned long long slot = list[i];
     // every field of both lines is loaded at once: a row's accumulators are
     // zero unless its flags say they were written, so no load waits on another
     const uint32_t m = (uint32_t)(*row_tag(tv, slot) & 0xFF);
@@ -108,12 +111,13 @@ __device__ __forceinline__ void apply_rows(const GameParams& G, const TableView&
       wide_rows += (flags & (kFlagDa | kFlagDs)) ? 1u : 0u;
     }
   }
+  }
   wide_rows = __reduce_add_sync(0xFFFFFFFFu, wide_rows);
-  if ((threadIdx.x & 31) == 0 && wide_rows) atomicAdd(tv.n_touched + 2 + (uid & 1), wide_rows);
+  if ((threadIdx.x & 31) == 0 && wide_rows) atomicAdd(wide_count(tv, uid & 1), wide_rows);
   if (leader) {
     const uint32_t next = (uid + 1) & 1;
-    tv.n_touched[next] = 0;
-    tv.n_touched[2 + next] = 0;
+    for (int sh = 0; sh < kListShards; ++sh) *list_count(tv, next, sh) = 0;
+    *wide_count(tv, next) = 0;
   }
 }
 
@@ -538,6 +542,19 @@ int check_device_error(mccfr_handle* h) {
       return fail(h, MCCFR_ERR_TABLE_FULL, "info-set table full (capacity %llu rows); raise table_log2", h->cap);
     return fail(h, MCCFR_ERR_DEVICE, "kernel error flags 0x%x", e);
   }
+  return MCCFR_OK;
+}
+
+// Rows the player-update of parity `par` listed (all shards) and folded wide.
+int read_touched(mccfr_handle* h, uint32_t par) {
+  unsigned c[kCounterBytes / 4];
+  CK(cudaMemcpy(c, h->tv.n_touched, sizeof(c), cudaMemcpyDeviceToHost));
+  TableView hv = h->tv;
+  hv.n_touched = c;
+  long long n = 0;
+  for (int sh = 0; sh < kListShards; ++sh) n += *list_count(hv, par, sh);
+  h->touched_last = n;
+  h->wide_last = *wide_count(hv, par);
   return MCCFR_OK;
 }
 
@@ -1054,7 +1071,7 @@ int mccfr_create(const mccfr_config* cfg, mccfr_handle** out) {
   // Table rows, the touched list and small counters in one allocation.
   h->cap = 1ull << cfg->table_log2;
   const unsigned long long C = h->cap;
-  const size_t bytes_rows = C * kRowBytes, bytes_touch = C * 4, bytes_misc = 256;
+  const size_t bytes_rows = C * kRowBytes, bytes_touch = C * 4, bytes_misc = kCounterBytes;
   h->block_bytes = bytes_rows + bytes_touch + bytes_misc;
   CKC(cudaMalloc(&h->d_block, bytes_rows + bytes_touch + bytes_misc));
   CKC(cudaMemset(h->d_block, 0, bytes_rows + bytes_touch + bytes_misc));
@@ -1063,7 +1080,7 @@ int mccfr_create(const mccfr_config* cfg, mccfr_handle** out) {
   h->tv.touched = reinterpret_cast<unsigned int*>(base + bytes_rows);
   char* misc = base + bytes_rows + bytes_touch;
   h->tv.n_touched = reinterpret_cast<unsigned int*>(misc);
-  h->tv.err = reinterpret_cast<int*>(misc + 64);
+  h->tv.err = reinterpret_cast<int*>(misc + kCounterBytes - 128);
   h->tv.mask = C - 1;
   h->tv.log2cap = cfg->table_log2;
   h->tv.direct = direct_map(*cfg);
@@ -1212,12 +1229,8 @@ int mccfr_step(mccfr_handle* h, long long iteration, int player, int batch, mccf
     h->traverse_ms += t1;
     h->apply_ms += t2;
     h->launches++;
-    unsigned nt[4] = {0, 0, 0, 0};
-    cudaMemcpy(nt, h->tv.n_touched, sizeof(nt), cudaMemcpyDeviceToHost);
     // the apply kernel resets the other parity's counters, not this one's
-    const uint32_t par = (uint32_t)((iteration - 1) * h->cfg.num_players + player) & 1;
-    h->touched_last = nt[par];
-    h->wide_last = nt[2 + par];
+    read_touched(h, (uint32_t)((iteration - 1) * h->cfg.num_players + player) & 1);
     rc = check_device_error(h);
   }
   if (rc == MCCFR_OK && trace) {
@@ -1259,11 +1272,7 @@ int mccfr_train(mccfr_handle* h, long long iters, int batch, int verbose, const 
       if (i + 1 == iters) {
         // rows touched by this iteration's last player-update (its parity's counter
         // is reset only by the next update's apply)
-        unsigned nt[4] = {0, 0, 0, 0};
-        CK(cudaMemcpy(nt, h->tv.n_touched, sizeof(nt), cudaMemcpyDeviceToHost));
-        const uint32_t par = (uint32_t)((base + i) * np + np - 1) & 1;
-        h->touched_last = nt[par];
-        h->wide_last = nt[2 + par];
+        if (read_touched(h, (uint32_t)((base + i) * np + np - 1) & 1)) return MCCFR_ERR_CUDA;
       }
     }
     h->launches += h->cfg.num_players;
@@ -1698,13 +1707,13 @@ int mccfr_level_counts(mccfr_handle* h, uint32_t* seeds, uint32_t* nodes, int ca
   if (deferred) *deferred = 0;
   if (!h->d_level) return MCCFR_OK;
   CK(cudaSetDevice(h->device));
-  LevelCtl c;
+  static thread_local LevelCtl c;
   CK(cudaMemcpyAsync(&c, h->lb.ctl, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   *levels = h->lb.nlev;
   for (int L = 0; L < h->lb.nlev && L < cap; ++L) {
-    seeds[L] = L == 0 ? (uint32_t)h->level_last_batch : c.seed_count[L];
-    nodes[L] = c.node_count[L];
+    seeds[L] = L == 0 ? (uint32_t)h->level_last_batch : level_seeds(c, L);
+    nodes[L] = level_nodes(c, L);
   }
   if (deferred) *deferred = c.deferred;
   return MCCFR_OK;

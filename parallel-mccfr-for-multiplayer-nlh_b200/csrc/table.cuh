@@ -29,11 +29,18 @@ constexpr int kOffKey = 0, kOffTag = 8, kOffCnt = 16, kOffSu = 24, kOffReg = 32,
               kOffDs = 160, kOffVisits = 224, kOffFlags = 232;
 constexpr unsigned kFlagDs = 1u, kFlagDa = 2u;
 
+// The touched-row list is cut into kListShards shards by the slot's low bits:
+// shard s holds slots s, s + S, s + 2S, ..., so it never holds more than cap / S
+// rows, and appends spread over S counters instead of queueing on one address.
+constexpr int kListShards = 32;
+constexpr int kCounterStride = 32;  // counters 128 bytes apart (separate lines)
+
 struct TableView {
   unsigned char* rows;       // [cap][256]
-  unsigned int* touched;     // [cap] rows touched by the update, in order of first touch
-  // [4], each pair by update-id parity: entries of `touched`, and rows whose
-  // second line the apply kernel folded
+  unsigned int* touched;     // [kListShards][cap / kListShards] rows touched by the update
+  // counters, kCounterStride words apart: entries of each shard by update-id
+  // parity (index parity * kListShards + shard), then, by parity, rows whose
+  // second line the apply kernel folded (index 2 * kListShards + parity)
   unsigned int* n_touched;
   unsigned long long mask;   // cap - 1
   int log2cap;
@@ -138,18 +145,29 @@ __device__ __forceinline__ long long table_insert(const TableView& tv, unsigned 
   return -1;
 }
 
+__host__ __device__ __forceinline__ unsigned int* list_count(const TableView& tv, uint32_t parity, int shard) {
+  return tv.n_touched + (size_t)kCounterStride * (parity * kListShards + shard);
+}
+__host__ __device__ __forceinline__ unsigned int* wide_count(const TableView& tv, uint32_t parity) {
+  return tv.n_touched + (size_t)kCounterStride * (2 * kListShards + parity);
+}
+// Bytes of the counter block (list counters, wide-row counters, error flag).
+constexpr size_t kCounterBytes = (size_t)kCounterStride * 4 * (2 * kListShards + 2) + 128;
+
 __device__ __forceinline__ void list_row(const TableView& tv, unsigned long long slot, uint32_t uid) {
-  const unsigned int i = atomicAdd(tv.n_touched + (uid & 1), 1u);
-  tv.touched[i] = (unsigned int)slot;
+  const int shard = (int)(slot & (kListShards - 1));
+  const unsigned int i = atomicAdd(list_count(tv, uid & 1, shard), 1u);
+  tv.touched[(size_t)shard * ((tv.mask + 1) / kListShards) + i] = (unsigned int)slot;
 }
 
 // Marks the row as touched by update `uid`; returns whether `vm` is the
-// update's canonical mask for that row (the first visitor sets it).
-__device__ __forceinline__ bool touch_row(const TableView& tv, unsigned long long slot, uint32_t uid,
-                                          uint32_t vm) {
+// update's canonical mask for that row (the first visitor sets it).  `old` is
+// the row's tag as the caller read it (any earlier value will do: a stale one
+// only makes the compare-and-swap fail and return the current tag).
+__device__ __forceinline__ bool touch_row_from(const TableView& tv, unsigned long long slot, uint32_t uid,
+                                               uint32_t vm, unsigned long long old) {
   const unsigned long long want = ((unsigned long long)(uid + 1) << 8) | vm;
   unsigned long long* tag = row_tag(tv, slot);
-  unsigned long long old = __ldcg(tag);
   if ((old >> 8) != (unsigned long long)(uid + 1)) {
     const unsigned long long r = atomicCAS(tag, old, want);
     if (r == old) {
@@ -159,6 +177,10 @@ __device__ __forceinline__ bool touch_row(const TableView& tv, unsigned long lon
     old = r;
   }
   return (uint32_t)(old & 0xFF) == vm;
+}
+__device__ __forceinline__ bool touch_row(const TableView& tv, unsigned long long slot, uint32_t uid,
+                                          uint32_t vm) {
+  return touch_row_from(tv, slot, uid, vm, __ldcg(row_tag(tv, slot)));
 }
 
 // Marks the row as touched by update `uid` without claiming a canonical mask

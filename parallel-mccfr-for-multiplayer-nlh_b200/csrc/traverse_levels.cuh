@@ -51,15 +51,29 @@ constexpr int kMaxLevels = 32;
 constexpr uint32_t kSeedDeferred = 0x80000000u;  // walked by the dfs kernel
 constexpr uint32_t kSeedInvalid = 0xFFFFFFFFu;   // child of a node that found no row (table full)
 
-// Per-update counters of the level arrays (zeroed before every update).
+// Per-update counters of the level arrays (zeroed before every update), each on
+// a 128-byte line of its own: every warp of a level's launch adds to them.
 struct LevelCtl {
-  uint32_t seed_count[kMaxLevels];  // seeds of level L (level 0: unused, the batch)
-  uint32_t node_count[kMaxLevels];  // updating-player nodes reached from level L
-  uint32_t grab[kMaxLevels];        // expand work counters
+  // level L: (updating-player nodes reached from level L << 32) | seeds of
+  // level L + 1, both bump-allocated by one 64-bit add
+  unsigned long long alloc[kMaxLevels][16];
+  uint32_t grab[kMaxLevels][32];    // expand work counters
   uint32_t deferred;                // seeds left to the dfs kernel
+  uint32_t pad0[31];
   uint32_t dfs_grab;
-  uint32_t pad[2];
+  uint32_t pad1[31];
 };
+__host__ __device__ __forceinline__ uint32_t level_nodes(const LevelCtl& c, int L) {
+  return (uint32_t)(c.alloc[L][0] >> 32);
+}
+// Seeds of level L >= 1 (level 0 holds the batch's roots).
+__host__ __device__ __forceinline__ uint32_t level_seeds(const LevelCtl& c, int L) {
+  return (uint32_t)c.alloc[L - 1][0];
+}
+
+// Seeds a warp takes from a level's work counter at a time (one atomic per
+// chunk instead of one per refill).
+constexpr uint32_t kGrabChunk = 32;
 
 struct LevelBufs {
   EsState* nodes;     // [node_cap] state at the node (aux = traversal index)
@@ -80,11 +94,11 @@ __device__ __forceinline__ LevelBase level_base(const LevelBufs& lb, int L, int 
   LevelBase b;
   uint32_t s = 0, n = 0;
   for (int l = 0; l < L; ++l) {
-    s += l == 0 ? (uint32_t)batch : lb.ctl->seed_count[l];
-    n += lb.ctl->node_count[l];
+    s += l == 0 ? (uint32_t)batch : level_seeds(*lb.ctl, l);
+    n += level_nodes(*lb.ctl, l);
   }
   b.seed = s;
-  b.count = L == 0 ? (uint32_t)batch : lb.ctl->seed_count[L];
+  b.count = L == 0 ? (uint32_t)batch : level_seeds(*lb.ctl, L);
   b.seed_next = s + b.count;
   b.node = n;
   return b;
@@ -192,8 +206,35 @@ __device__ __forceinline__ int lv_step(const GameParams& G, const TableView& tv,
     bkt = cur.street ? ((cw >> (8 * cur.street)) & 0xFF) : 0u;
   }
   const unsigned long long key = info_key(G, player, hb, bkt, cur.street, cur.abits, cur.path);
-  const long long slot = table_insert<W>(tv, key);
   cnt.visits++;
+  if (tv.direct) {
+    // key k owns row k-1: the updating player's row is read (and its key
+    // stored) by the back pass; an opponent's key, tag and regrets are loaded
+    // together, and its draw is computed while they are in flight
+    const unsigned long long rs = key - 1;
+    if (player == up) {
+      vm_out = vm;
+      slot_out = (long long)rs;
+      return kLvUp;
+    }
+    const ulonglong2 kt = __ldcg(reinterpret_cast<const ulonglong2*>(row_ptr(tv, rs)));
+    const float4* rp = row_reg(tv, rs);
+    const float4 r0 = __ldg(rp), r1 = __ldg(rp + 1);
+    const U4 d = philox(U4{cur.aux, uid, (uint32_t)cur.path, (uint32_t)(cur.path >> 32) | 0x80000000u},
+                        G.seed_lo, G.seed_hi);
+    if (kt.x != key) __stcg(row_key(tv, rs), key);
+    const float reg[kSlots] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
+    const int s = sample_action(G, reg, vm, uniform01(d.x));
+    if (touch_row_from(tv, rs, uid, vm, kt.y)) {
+      atomicAdd(row_cnt(tv, rs), (1ull << 32) | 1ull);
+    } else {
+      lv_off_canonical(tv, rs, vm, reg);
+    }
+    pend.player = player;
+    pend.action = s;
+    return kLvGoOn;
+  }
+  const long long slot = table_insert<W>(tv, key);
   if (player == up) {
     vm_out = vm;
     slot_out = slot;
@@ -273,8 +314,8 @@ k_level_expand(const GameParams G, const TableView tv, const DealRec* __restrict
   const uint32_t holders = min((uint32_t)(gridDim.x * BLOCK), B.count);
   const unsigned long long need_nodes = (unsigned long long)B.node + holders;
   const unsigned long long need_seeds = (unsigned long long)B.seed_next + (unsigned long long)holders * G.num_actions;
-  uint32_t* node_count = lb.ctl->node_count + L;
-  uint32_t* next_count = lb.ctl->seed_count + (last ? L : L + 1);
+  unsigned long long* alloc = &lb.ctl->alloc[L][0];
+  uint32_t* grab = &lb.ctl->grab[L][0];
   EsCounts c{0, 0, 0};
   unsigned trav = 0, deferred = 0;
   EsState cur;
@@ -282,17 +323,23 @@ k_level_expand(const GameParams G, const TableView tv, const DealRec* __restrict
   LvPending pend{-1, 0};
   uint32_t seed = 0;
   bool have = false, more = true;
+  // the warp's seeds not yet handed out: [pool, pool_end) of the level
+  uint32_t pool = 0, pool_end = 0;
   for (;;) {
     __syncwarp();
     const bool need = !have && more;
     const unsigned needm = __ballot_sync(0xFFFFFFFFu, need);
     if (needm) {
-      const int leader = __ffs(needm) - 1;
-      unsigned base = 0;
-      if (lane == leader) base = atomicAdd(lb.ctl->grab + L, (unsigned)__popc(needm));
-      base = __shfl_sync(0xFFFFFFFFu, base, leader);
+      const uint32_t k = (uint32_t)__popc(needm);
+      const uint32_t avail = pool_end - pool;
+      uint32_t chunk = 0;
+      if (avail < k) {
+        if (lane == 0) chunk = atomicAdd(grab, kGrabChunk);
+        chunk = __shfl_sync(0xFFFFFFFFu, chunk, 0);
+      }
       if (need) {
-        const uint32_t i = base + (uint32_t)__popc(needm & ((1u << lane) - 1u));
+        const uint32_t rank = (uint32_t)__popc(needm & ((1u << lane) - 1u));
+        const uint32_t i = rank < avail ? pool + rank : chunk + (rank - avail);
         if (i >= B.count) {
           more = false;
         } else {
@@ -300,8 +347,8 @@ k_level_expand(const GameParams G, const TableView tv, const DealRec* __restrict
           const uint32_t w = ROOT ? 0u : __ldcg(lb.child + seed);
           bool ok = w != kSeedInvalid && !last;
           if (ok) {
-            ok = need_nodes + ld_volatile(node_count) <= lb.node_cap &&
-                 need_seeds + ld_volatile(next_count) <= lb.seed_cap;
+            const unsigned long long a = *(volatile const unsigned long long*)alloc;
+            ok = need_nodes + (a >> 32) <= lb.node_cap && need_seeds + (uint32_t)a <= lb.seed_cap;
           }
           if (w == kSeedInvalid) {
             // child of a node that found no row: nothing to walk
@@ -319,6 +366,12 @@ k_level_expand(const GameParams G, const TableView tv, const DealRec* __restrict
             have = true;
           }
         }
+      }
+      if (avail >= k) {
+        pool += k;
+      } else {
+        pool = chunk + (k - avail);
+        pool_end = chunk + kGrabChunk;
       }
     }
     if (!__any_sync(0xFFFFFFFFu, have || more)) break;
@@ -346,13 +399,10 @@ k_level_expand(const GameParams G, const TableView tv, const DealRec* __restrict
         if (lane >= o) incl += y;
       }
       const int total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-      unsigned jn = 0, jc = 0;
-      if (lane == 0) {
-        jn = atomicAdd(node_count, (unsigned)__popc(upm));
-        jc = atomicAdd(next_count, (unsigned)total);
-      }
-      jn = __shfl_sync(0xFFFFFFFFu, jn, 0);
-      jc = __shfl_sync(0xFFFFFFFFu, jc, 0);
+      unsigned long long j2 = 0;
+      if (lane == 0) j2 = atomicAdd(alloc, ((unsigned long long)__popc(upm) << 32) | (unsigned)total);
+      j2 = __shfl_sync(0xFFFFFFFFu, j2, 0);
+      const uint32_t jn = (uint32_t)(j2 >> 32), jc = (uint32_t)j2;
       if (isup) {
         const uint32_t j = B.node + jn + (uint32_t)__popc(upm & ((1u << lane) - 1u));
         const uint32_t cb = B.seed_next + jc + (uint32_t)(incl - k);
@@ -460,7 +510,7 @@ template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 k_level_back(const GameParams G, const TableView tv, const Sched* __restrict__ sched, int batch, float rscale,
              const LevelBufs lb, int L, Counters* __restrict__ counters) {
-  const uint32_t n = lb.ctl->node_count[L];
+  const uint32_t n = level_nodes(*lb.ctl, L);
   if (n == 0) return;
   __shared__ LevelBase s_base;
   if (threadIdx.x == 0) s_base = level_base(lb, L, batch);
@@ -473,7 +523,12 @@ k_level_back(const GameParams G, const TableView tv, const Sched* __restrict__ s
     const uint32_t vm = m.w;
     if (!vm) continue;
     const unsigned long long slot = m.x;
-    // independent of each other: the claim, the row's regrets, the children's values
+    // independent of each other: the claim, the row's regrets, the children's
+    // values, and (direct map) the row's key, which the expand pass left to this pass
+    if (tv.direct) {
+      const unsigned long long k = __ldcg(row_key(tv, slot));
+      if (k != slot + 1) __stcg(row_key(tv, slot), slot + 1);
+    }
     claim_row(tv, slot, uid);
     float reg[kSlots], strat[kSlots], v[kSlots];
     load_regrets(tv, (long long)slot, reg);
