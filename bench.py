@@ -868,9 +868,11 @@ def main():
     elif tr_prof and "dram_bytes_per_traversal" in tr_prof:
         traffic = tr_prof["dram_bytes_per_traversal"] * (trav / launches)
     if level_form:
-        kernel_name = "k_level_expand + k_level_dfs + k_level_back (the traversal of one player-update)"
-        # per update: k_deal, nlev expand levels, k_level_dfs, nlev-1 back levels, k_apply, k_advance
-        launches_per_update = 2 * nlev + 3
+        kernel_name = ("k_level_expand + k_level_dfs + k_level_showdown + k_level_back (the traversal of one "
+                       "player-update)")
+        # per update: k_deal, nlev expand levels, k_level_dfs, k_level_showdown, nlev-1 back levels,
+        # k_apply, k_advance
+        launches_per_update = 2 * nlev + 4
     else:
         kernel_name = "k_traverse_es" if cfg.sampling == 1 else "k_traverse_ref"
         launches_per_update = 4  # k_deal, the traversal, k_apply, k_advance

@@ -622,9 +622,10 @@ int level_count(const mccfr_handle* h) {
 }
 
 // Node and seed buffers for updates of `batch` traversals: 2^level_log2 node
-// records of 80 B (default: 64 per traversal, 2^18..2^26) and 8 seeds of 8 B
-// per node (at least the batch and a margin).  A smaller allocation is tried when the
-// device is short of memory; any size gives the same rows.
+// records of 80 B (default: 64 per traversal, 2^18..2^26), 8 seeds of 8 B per
+// node (at least the batch and a margin) and one 24-byte showdown record per
+// node.  A smaller allocation is tried when the device is short of memory; any
+// size gives the same rows.
 int ensure_levels(mccfr_handle* h, int batch) {
   const int nlev = level_count(h);
   if (h->d_level && h->level_batch >= batch) {
@@ -650,7 +651,9 @@ int ensure_levels(mccfr_handle* h, int batch) {
   for (;; --lg) {
     const unsigned long long nodes = 1ull << lg;
     const unsigned long long seeds = std::max(8ull * nodes, (unsigned long long)batch + (1ull << 20));
-    const size_t bytes = nodes * (sizeof(EsState) + sizeof(uint4)) + seeds * 8 + sizeof(LevelCtl) + 256;
+    const unsigned long long shows = nodes;
+    const size_t bytes =
+        nodes * (sizeof(EsState) + sizeof(uint4)) + seeds * 8 + shows * sizeof(ShowRec) + sizeof(LevelCtl) + 256;
     const cudaError_t e = cudaMalloc(&h->d_level, bytes);
     if (e == cudaSuccess) {
       char* p = static_cast<char*>(h->d_level);
@@ -662,9 +665,13 @@ int ensure_levels(mccfr_handle* h, int batch) {
       p += seeds * 4;
       h->lb.value = reinterpret_cast<float*>(p);
       p += seeds * 4;
+      h->lb.show = reinterpret_cast<ShowRec*>(p);
+      p += shows * sizeof(ShowRec);
+      p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 127) & ~(uintptr_t)127);
       h->lb.ctl = reinterpret_cast<LevelCtl*>(p);
       h->lb.node_cap = (uint32_t)nodes;
       h->lb.seed_cap = (uint32_t)seeds;
+      h->lb.show_cap = (uint32_t)shows;
       h->level_bytes = bytes;
       h->level_batch = batch;
       break;
@@ -695,8 +702,8 @@ int ensure_levels(mccfr_handle* h, int batch) {
 }
 
 // One external-sampling update in the level-synchronous form: the levels
-// expanded top down, the seeds that did not fit walked depth first, the values
-// returned bottom up.
+// expanded top down, the seeds that did not fit walked depth first, the
+// recorded showdowns evaluated in one pass, the values returned bottom up.
 int enqueue_levels(mccfr_handle* h, int batch, float rscale) {
   const LevelBufs& lb = h->lb;
   h->level_last_batch = batch;
@@ -709,6 +716,8 @@ int enqueue_levels(mccfr_handle* h, int batch, float rscale) {
   CK(cudaGetLastError());
   k_level_dfs<128, 2, 1><<<h->grid_dfs, 128, 2 * 128 * sizeof(EsFrame), h->stream>>>(
       h->gp, h->tv, h->d_deals, h->d_sched, batch, rscale, lb, h->d_counters);
+  CK(cudaGetLastError());
+  k_level_showdown<256><<<h->grid_back, 256, 0, h->stream>>>(h->gp, h->d_deals, h->d_sched, lb);
   CK(cudaGetLastError());
   for (int L = lb.nlev - 2; L >= 0; --L)
     k_level_back<256><<<h->grid_back, 256, 0, h->stream>>>(h->gp, h->tv, h->d_sched, batch, rscale, lb, L,

@@ -60,6 +60,8 @@ struct LevelCtl {
   uint32_t grab[kMaxLevels][32];    // expand work counters
   uint32_t deferred;                // seeds left to the dfs kernel
   uint32_t pad0[31];
+  uint32_t show_count;              // showdown records appended by the expand passes
+  uint32_t pad2[31];
   uint32_t dfs_grab;
   uint32_t pad1[31];
 };
@@ -72,16 +74,25 @@ __host__ __device__ __forceinline__ uint32_t level_seeds(const LevelCtl& c, int 
 }
 
 // Seeds a warp takes from a level's work counter at a time (one atomic per
-// chunk instead of one per refill).
+// chunk instead of one per refill), and the idle lanes a refill waits for.
 constexpr uint32_t kGrabChunk = 32;
+constexpr int kRefillMin = 8;
+
+// A showdown reached by an expand pass, evaluated by the batched showdown pass:
+// the seed whose value it is, the traversal, the folded players and the chips
+// each player put in (two per word).
+struct __align__(8) ShowRec {
+  uint32_t seed, aux, folded, inv01, inv23, inv45;
+};
 
 struct LevelBufs {
   EsState* nodes;     // [node_cap] state at the node (aux = traversal index)
   uint4* meta;        // [node_cap] {row slot, own seed, first child seed, legal mask (0: none)}
   uint32_t* child;    // [seed_cap] (node << 3) | action; kSeedDeferred / kSeedInvalid marks
   float* value;       // [seed_cap] the seed's value for the updating player
+  ShowRec* show;      // [show_cap] showdowns left to the batched pass
   LevelCtl* ctl;
-  uint32_t node_cap, seed_cap;
+  uint32_t node_cap, seed_cap, show_cap;
   int nlev;           // seed levels (the last one is left to the dfs kernel)
 };
 
@@ -104,7 +115,7 @@ __device__ __forceinline__ LevelBase level_base(const LevelBufs& lb, int L, int 
   return b;
 }
 
-enum { kLvGoOn = 0, kLvDone = 1, kLvUp = 2 };
+enum { kLvGoOn = 0, kLvDone = 1, kLvUp = 2, kLvShow = 3 };
 
 // Side-pot showdown payoff of the updating player (side_pot_payoff), kept out
 // of line so that the loop the lanes share stays small in the instruction
@@ -140,14 +151,15 @@ struct LvPending {
 };
 
 // One step of a seed's walk (the descend branch of es_step): the pending action,
-// the cheap steps (depth cut, fold win, street change, showdown), then at most
-// one decision node.  An opponent's node is done here (its sampled action is
-// left pending); at an updating-player node the walk stops with the node's mask
-// and row slot (its regrets are read in back).
+// the cheap steps (depth cut, fold win, street change), then a showdown (its
+// folded players and chips handed back in `sd` for the batched showdown pass)
+// or at most one decision node.  An opponent's node is done here (its sampled
+// action is left pending); at an updating-player node the walk stops with the
+// node's mask and row slot (its regrets are read in back).
 template <int W>
 __device__ __forceinline__ int lv_step(const GameParams& G, const TableView& tv, uint32_t uid, int up, EsState& cur,
                                        const DealRec* D, LvPending& pend, float& value, uint32_t& vm_out,
-                                       long long& slot_out, EsCounts& cnt) {
+                                       long long& slot_out, uint4& sd, EsCounts& cnt) {
   const int N = G.N;
   const uint32_t all_players = (1u << N) - 1;
   if (pend.player >= 0) {
@@ -187,11 +199,11 @@ __device__ __forceinline__ int lv_step(const GameParams& G, const TableView& tv,
         continue;
       }
     }
-    value = lv_showdown(N, up, cur.folded, (uint32_t)cur.inv[0] | ((uint32_t)cur.inv[1] << 16),
-                        (uint32_t)cur.inv[2] | ((uint32_t)cur.inv[3] << 16),
-                        (uint32_t)cur.inv[4] | ((uint32_t)cur.inv[5] << 16), D);
+    sd = make_uint4((uint32_t)cur.folded, (uint32_t)cur.inv[0] | ((uint32_t)cur.inv[1] << 16),
+                    (uint32_t)cur.inv[2] | ((uint32_t)cur.inv[3] << 16),
+                    (uint32_t)cur.inv[4] | ((uint32_t)cur.inv[5] << 16));
     cnt.terminals++;
-    return kLvDone;
+    return kLvShow;
   }
   const int player = (int)(cur.q & 0xF);
   const int to_call = cur.cb - pget(cur.bet, player);
@@ -323,28 +335,39 @@ k_level_expand(const GameParams G, const TableView tv, const DealRec* __restrict
   LvPending pend{-1, 0};
   uint32_t seed = 0;
   bool have = false, more = true;
-  // the warp's seeds not yet handed out: [pool, pool_end) of the level
-  uint32_t pool = 0, pool_end = 0;
+  // The warp's seeds not yet handed out, [pool, pool_end): one chunk of
+  // kGrabChunk seeds of the level, whose child words were loaded (one per lane,
+  // `pw`) when the chunk was taken.  Idle lanes are refilled together, once at
+  // least kRefillMin of them wait or none has work: a refill stalls the warp on
+  // the new seeds' parent records, so fewer refills stall it less often.
+  uint32_t pool = 0, pool_end = 0, pw = 0;
   for (;;) {
     __syncwarp();
     const bool need = !have && more;
     const unsigned needm = __ballot_sync(0xFFFFFFFFu, need);
-    if (needm) {
-      const uint32_t k = (uint32_t)__popc(needm);
-      const uint32_t avail = pool_end - pool;
-      uint32_t chunk = 0;
-      if (avail < k) {
+    const unsigned busym = __ballot_sync(0xFFFFFFFFu, have);
+    if (needm && (__popc(needm) >= kRefillMin || !busym)) {
+      uint32_t avail = pool_end - pool;
+      if (avail == 0) {
+        uint32_t chunk = 0;
         if (lane == 0) chunk = atomicAdd(grab, kGrabChunk);
         chunk = __shfl_sync(0xFFFFFFFFu, chunk, 0);
+        pool = chunk;
+        pool_end = chunk + kGrabChunk;
+        avail = kGrabChunk;
+        if (!ROOT) pw = chunk + (uint32_t)lane < B.count ? __ldcg(lb.child + B.seed + chunk + lane) : kSeedInvalid;
       }
-      if (need) {
-        const uint32_t rank = (uint32_t)__popc(needm & ((1u << lane) - 1u));
-        const uint32_t i = rank < avail ? pool + rank : chunk + (rank - avail);
+      const uint32_t k = (uint32_t)__popc(needm);
+      const uint32_t take = min(k, avail);
+      const uint32_t rank = (uint32_t)__popc(needm & ((1u << lane) - 1u));
+      const uint32_t i = pool + rank;
+      const uint32_t wl = ROOT ? 0u : __shfl_sync(0xFFFFFFFFu, pw, (int)((i - (pool_end - kGrabChunk)) & 31u));
+      if (need && rank < take) {
         if (i >= B.count) {
           more = false;
         } else {
           seed = B.seed + i;
-          const uint32_t w = ROOT ? 0u : __ldcg(lb.child + seed);
+          const uint32_t w = wl;
           bool ok = w != kSeedInvalid && !last;
           if (ok) {
             const unsigned long long a = *(volatile const unsigned long long*)alloc;
@@ -367,22 +390,36 @@ k_level_expand(const GameParams G, const TableView tv, const DealRec* __restrict
           }
         }
       }
-      if (avail >= k) {
-        pool += k;
-      } else {
-        pool = chunk + (k - avail);
-        pool_end = chunk + kGrabChunk;
-      }
+      pool += take;
     }
     if (!__any_sync(0xFFFFFFFFu, have || more)) break;
     int r = -1;
     uint32_t vm = 0;
     long long slot = -1;
     float v = 0.0f;
+    uint4 sd = make_uint4(0u, 0u, 0u, 0u);
     if (have) {
-      r = lv_step<W>(G, tv, uid, up, cur, D, pend, v, vm, slot, c);
+      r = lv_step<W>(G, tv, uid, up, cur, D, pend, v, vm, slot, sd, c);
       if (r == kLvDone) {
         lb.value[seed] = v;
+        have = false;
+      }
+    }
+    // showdowns of this step: one record each for the batched showdown pass
+    // (computed here when the record list is full)
+    const bool issd = have && r == kLvShow;
+    const unsigned sdm = __ballot_sync(0xFFFFFFFFu, issd);
+    if (sdm) {
+      uint32_t sb = 0;
+      if (lane == 0) sb = atomicAdd(&lb.ctl->show_count, (unsigned)__popc(sdm));
+      sb = __shfl_sync(0xFFFFFFFFu, sb, 0);
+      if (issd) {
+        const uint32_t j = sb + (uint32_t)__popc(sdm & ((1u << lane) - 1u));
+        if (j < lb.show_cap) {
+          lb.show[j] = ShowRec{seed, cur.aux, sd.x, sd.y, sd.z, sd.w};
+        } else {
+          lb.value[seed] = lv_showdown(G.N, up, sd.x, sd.y, sd.z, sd.w, D);
+        }
         have = false;
       }
     }
@@ -504,6 +541,20 @@ k_level_dfs(const GameParams G, const TableView tv, const DealRec* __restrict__ 
     }
   }
   warp_add_counters(counters, trav, c.visits, c.updates, c.terminals, trav * (unsigned)G.N);
+}
+
+// The showdowns the expand passes recorded, one thread each: all lanes of a
+// warp run the same side-pot arithmetic (side_pot_payoff) on their own record.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_level_showdown(const GameParams G, const DealRec* __restrict__ deals, const Sched* __restrict__ sched,
+                 const LevelBufs lb) {
+  const uint32_t n = min(ld_volatile(&lb.ctl->show_count), lb.show_cap);
+  const int up = sched->player;
+  for (uint32_t i = blockIdx.x * BLOCK + threadIdx.x; i < n; i += gridDim.x * BLOCK) {
+    const ShowRec r = lb.show[i];
+    lb.value[r.seed] = lv_showdown(G.N, up, r.folded, r.inv01, r.inv23, r.inv45, deals + r.aux);
+  }
 }
 
 template <int BLOCK>
