@@ -119,9 +119,11 @@ typedef struct mccfr_config {
      not part of the game (a v2 checkpoint loads into any form). */
   int32_t traversal_form;
   /* MCCFR_FORM_LEVELS only: capacity of the updating-player node buffer as
-     log2 of the node records (80 B each; the child buffer holds eight times as
-     many 12 B entries); 0 = sized from the batch.  Subtrees that do not fit are
-     walked depth first inside the same update, with the same result. */
+     log2 of the node records (80 B each; the seed buffer holds eight times as
+     many 8 B entries, the showdown buffer one 24 B record per node); 0 = sized
+     from the batch.  Subtrees that do not fit are walked depth first inside the
+     same update, and showdowns that do not fit are evaluated where they are
+     reached, with the same result. */
   int32_t level_log2;
   int32_t reserved[5];
 } mccfr_config;
