@@ -95,6 +95,36 @@ def test_full_size_update_equals_oracle(hand_table, form):
     orc.close()
 
 
+@pytest.mark.parametrize("lg", [8, 14, 16])
+def test_level_buffers_smaller_than_the_update(hand_table, lg):
+    """The level form with node buffers far below its default of 64 per
+    traversal (2^lg node records for 4,096 traversals, and as many showdown
+    records): a seed that may not fit is left to the depth-first kernel (at
+    lg = 8 every root is, at lg = 14 the levels below the first), and a showdown
+    past the end of its record list is evaluated where it is reached (at
+    iteration 1 a traversal reaches more showdowns than lg = 16 leaves records
+    for).  Three iterations from an empty table; the table digest equals the
+    oracle's after each, and every row after the last."""
+    cfg = L.preset(L.PRESET_6MAX_100BB)
+    cfg.table_log2, cfg.key_bits = 22, 21
+    cfg.traversal_form = L.FORM_LEVELS
+    cfg.level_log2 = lg
+    tr = trainer(cfg, hand_table)
+    orc = binding.Oracle(cfg, hand_table)
+    for it in range(1, 4):
+        tr.train(1, 4096, verbose=False)
+        orc.train(1, 4096, threads=THREADS)
+        assert tr.digest() == orc.digest(), f"iteration {it}"
+    assert_rows_equal(tr.export_rows(), orc.export_rows())
+    lv = tr.level_counts()
+    if lg <= 14:
+        assert lv["deferred"] > 0
+    st, oc = tr.stats(), orc.counters()
+    assert (st.node_visits, st.traverser_updates, st.terminals) == (oc["visits"], oc["updates"], oc["terminals"])
+    tr.close()
+    orc.close()
+
+
 def uneven_tables():
     """Four tables of different shapes: 2, 3, 4 and 6 players; stacks 20, 50,
     80 and 150BB; 4, 3, 5 and 6 action slots; per-update traversals uneven."""
