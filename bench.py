@@ -405,6 +405,27 @@ def multitable_configs(L, n_tables=64, seed=2, scale=16):
     return out
 
 
+def time_table_graphs(m, L, make, counts, iters) -> float:
+    """Wall-clock seconds of `iters` iterations of a fresh set of tables trained
+    as one batch in the table-graph form (every table's own update kernels as a
+    concurrent branch of one graph per iteration), after one untimed iteration."""
+    import torch
+
+    ts = make()
+    g = m.Batch(ts, counts)
+    g.set_tuning(form=L.BATCH_TABLE_GRAPHS)
+    g.train(1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g.train(iters)
+    torch.cuda.synchronize()
+    secs = time.perf_counter() - t0
+    g.close()
+    for t in ts:
+        t.close()
+    return secs
+
+
 def multitable(m, L, table, iters=2) -> dict:
     import torch
 
@@ -448,12 +469,16 @@ def multitable(m, L, table, iters=2) -> dict:
     b.close()
     for t in batched:
         t.close()
+    graphs_s = time_table_graphs(m, L, make, [n for _, n in specs], iters)
     trav = iters * sum(n * c.num_players for c, n in specs)
     return {"tables": len(specs), "traversals_per_iteration": trav // iters,
             "plain_traversals_per_s": trav / plain_s, "batched_traversals_per_s": trav / batched_s,
             "speedup": plain_s / batched_s, "tuning": best,
+            "table_graphs_traversals_per_s": trav / graphs_s, "table_graphs_speedup": plain_s / graphs_s,
             "workload": "64 tables, players U{2..6}, stacks U[10,200]BB, 3-6 actions, traversals/update "
-                        "LogNormal(14,1)/16, seed 2; wall clock over iterations 2-3 of fresh tables, both forms"}
+                        "LogNormal(14,1)/16, seed 2; wall clock over iterations 2-3 of fresh tables; plain "
+                        "(table after table), batched (one persistent launch per phase, autotuned) and "
+                        "table_graphs (every table's own kernels as concurrent branches of one graph)"}
 
 
 def batched_small_tables(m, L, table, n_tables=64, batch=4096, iters=3) -> dict:
@@ -461,9 +486,10 @@ def batched_small_tables(m, L, table, n_tables=64, batch=4096, iters=3) -> dict:
     (2^20-row tables, 20-bit keys, seeds 100..163) of 4,096 traversals per
     player-update each.  Plain: every table's iteration on its own (one graph
     replay each, the level-synchronous kernels), one table after another;
-    batched: all 64 in one persistent traversal launch per phase.  Both over the
-    same iterations of fresh tables, wall clock; rows are bit-identical between
-    the two (tests/test_gpu_batched.py)."""
+    batched: all 64 in one persistent traversal launch per phase; table graphs:
+    every table's own update kernels as concurrent branches of one graph per
+    iteration.  All over the same iterations of fresh tables, wall clock; rows
+    are bit-identical between the forms (tests/test_gpu_batched.py)."""
     import torch
 
     def make():
@@ -506,12 +532,14 @@ def batched_small_tables(m, L, table, n_tables=64, batch=4096, iters=3) -> dict:
     b.close()
     for t in batched:
         t.close()
+    graphs_s = time_table_graphs(m, L, make, [batch] * n_tables, iters)
     trav = iters * n_tables * batch * 6
     return {"tables": n_tables, "traversals_per_update": batch, "iterations": iters,
             "plain_traversals_per_s": trav / plain_s, "batched_traversals_per_s": trav / batched_s,
             "speedup": plain_s / batched_s, "tuning": best,
+            "table_graphs_traversals_per_s": trav / graphs_s, "table_graphs_speedup": plain_s / graphs_s,
             "workload": "64 tables of 6-max 100BB, 4,096 traversals per player-update each, iterations 2-4 of "
-                        "fresh tables, wall clock, both forms"}
+                        "fresh tables, wall clock; plain, batched (persistent) and table_graphs forms"}
 
 
 def serving_sweep(m, L, table, rates=(10, 30, 100, 300, 1000), n_requests=48) -> dict:

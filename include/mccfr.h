@@ -335,8 +335,17 @@ typedef struct mccfr_batch_tuning {
   int32_t warp_sync;      /* lanes that refill together share one grab of lanes x grab
                              traversals; 1: interleaved (neighbouring lanes take neighbouring
                              traversals), 0: each lane a contiguous run of `grab` */
-  int32_t reserved[3];
+  int32_t form;           /* MCCFR_BATCH_* (mccfr_batch_train only; rounds always run the
+                             persistent kernel) */
+  int32_t reserved[2];
 } mccfr_batch_tuning;
+/* Batch forms.  PERSISTENT: per phase one persistent traversal launch over all
+   tables (the fields above tune it).  TABLE_GRAPHS: each table's own update
+   kernels (for external sampling the level-synchronous form) as independent
+   branches of one CUDA graph per iteration, so the tables' launches run
+   concurrently; the tuning fields above are then unused.  Both give every
+   table the rows of training it alone. */
+enum { MCCFR_BATCH_PERSISTENT = 0, MCCFR_BATCH_TABLE_GRAPHS = 1 };
 typedef struct mccfr_batch_stats {
   int64_t iterations;
   int64_t traversals;       /* all tables */

@@ -1781,8 +1781,10 @@ struct mccfr_batch {
   DealRec* d_deals = nullptr;
   unsigned long long* d_work = nullptr;
   unsigned long long max_items = 0;
-  mccfr_batch_tuning tuning{128, 2, 0, 1, 1, {0, 0, 0}};
+  mccfr_batch_tuning tuning{128, 2, 0, 1, 1, MCCFR_BATCH_PERSISTENT, {0, 0}};
   cudaGraphExec_t graph = nullptr;
+  cudaEvent_t ev_fork = nullptr;       // table-graph form: fork and joins of the tables' branches
+  std::vector<cudaEvent_t> ev_join;
   cudaEvent_t ev_it[2] = {nullptr, nullptr};
   cudaEvent_t ev_ph[2 * MCCFR_MAX_PLAYERS] = {};
   long long iterations = 0;
@@ -1828,7 +1830,7 @@ BatchedKernel pick_kernel(const mccfr_batch_tuning& t) {
 bool valid_tuning(const mccfr_batch_tuning& t) {
   return (t.block == 64 || t.block == 128 || t.block == 256) && (t.grab == 1 || t.grab == 2 || t.grab == 4 || t.grab == 8) &&
          (t.smem_frames == 0 || t.smem_frames == 2 || t.smem_frames == 4) && (t.probe_width == 1 || t.probe_width == 2) &&
-         (t.warp_sync == 0 || t.warp_sync == 1);
+         (t.warp_sync == 0 || t.warp_sync == 1) && (t.form == MCCFR_BATCH_PERSISTENT || t.form == MCCFR_BATCH_TABLE_GRAPHS);
 }
 
 size_t batched_smem(const mccfr_batch_tuning& t) {
@@ -1870,6 +1872,49 @@ int batch_enqueue_iteration(mccfr_batch* b, bool capturing) {
     BCK(cudaGetLastError());
   }
   BCK(rec(b->ev_it[1]));
+  return MCCFR_OK;
+}
+
+// One iteration of every table, each on its own stream: the batch stream
+// forks into one branch per table (its N player-updates, as its own training
+// graph holds them) and joins them again, so that a capture of this is one
+// graph whose branches the device runs concurrently.  Buffers are sized first:
+// nothing may allocate while the stream is captured.
+int batch_enqueue_table_graphs(mccfr_batch* b, bool capturing) {
+  auto rec = [&](cudaEvent_t e, cudaStream_t s) {
+    return capturing ? cudaEventRecordWithFlags(e, s, cudaEventRecordExternal) : cudaEventRecord(e, s);
+  };
+  BCK(rec(b->ev_it[0], b->stream));
+  BCK(cudaEventRecord(b->ev_fork, b->stream));
+  for (size_t i = 0; i < b->tables.size(); ++i) {
+    mccfr_handle* h = b->tables[i];
+    BCK(cudaStreamWaitEvent(h->stream, b->ev_fork, 0));
+    for (int p = 0; p < h->cfg.num_players; ++p) {
+      const int rc = enqueue_update(h, b->traversals[i], nullptr, nullptr, capturing);
+      if (rc) return bfail(b, rc, "table update in the batch graph");
+      k_advance<<<1, 1, 0, h->stream>>>(h->d_sched, h->cfg.num_players);
+      BCK(cudaGetLastError());
+    }
+    BCK(cudaEventRecord(b->ev_join[i], h->stream));
+    BCK(cudaStreamWaitEvent(b->stream, b->ev_join[i], 0));
+  }
+  BCK(rec(b->ev_it[1], b->stream));
+  return MCCFR_OK;
+}
+
+int batch_prepare_table_graphs(mccfr_batch* b) {
+  if (!b->ev_fork) BCK(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+  while (b->ev_join.size() < b->tables.size()) {
+    cudaEvent_t e = nullptr;
+    BCK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b->ev_join.push_back(e);
+  }
+  for (size_t i = 0; i < b->tables.size(); ++i) {
+    mccfr_handle* h = b->tables[i];
+    int rc = ensure_deals(h, b->traversals[i]);
+    if (!rc && use_levels(h)) rc = ensure_levels(h, b->traversals[i]);
+    if (rc) return bfail(b, rc, "table buffers for the batch graph");
+  }
   return MCCFR_OK;
 }
 
@@ -1990,6 +2035,9 @@ void mccfr_batch_destroy(mccfr_batch* b) {
   if (!b) return;
   cudaSetDevice(b->device);
   if (b->graph) cudaGraphExecDestroy(b->graph);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  for (auto& e : b->ev_join)
+    if (e) cudaEventDestroy(e);
   for (auto& e : b->ev_it)
     if (e) cudaEventDestroy(e);
   for (auto& e : b->ev_ph)
@@ -2024,10 +2072,16 @@ int mccfr_batch_train(mccfr_batch* b, long long iters, int flags) {
   BCK(cudaSetDevice(b->device));
   int rc = batch_set_scheds(b);
   if (rc) return rc;
+  const bool tgraphs = b->tuning.form == MCCFR_BATCH_TABLE_GRAPHS;
+  if (!b->graph && tgraphs) {
+    rc = batch_prepare_table_graphs(b);
+    if (rc) return rc;
+    BCK(cudaStreamSynchronize(b->stream));
+  }
   if (!b->graph) {
     cudaGraph_t g = nullptr;
     BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    rc = batch_enqueue_iteration(b, true);
+    rc = tgraphs ? batch_enqueue_table_graphs(b, true) : batch_enqueue_iteration(b, true);
     const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     if (rc) {
       if (g) cudaGraphDestroy(g);
@@ -2043,7 +2097,12 @@ int mccfr_batch_train(mccfr_batch* b, long long iters, int flags) {
     BCK(cudaGraphLaunch(b->graph, b->stream));
     if (timed) {
       BCK(cudaEventSynchronize(b->ev_it[1]));
-      batch_time_phases(b);
+      if (tgraphs) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, b->ev_it[0], b->ev_it[1]) == cudaSuccess) b->total_ms += ms;
+      } else {
+        batch_time_phases(b);
+      }
     }
   }
   return batch_after(b, iters);
@@ -2058,7 +2117,7 @@ int mccfr_batch_autotune(mccfr_batch* b, int max_candidates, mccfr_batch_tuning*
     for (int grab : {1, 2, 4, 8})
       for (int k : {0, 2, 4})
         for (int ws : {1, 0})
-          for (int w : {1, 2}) cands.push_back(mccfr_batch_tuning{blk, grab, k, w, ws, {0, 0, 0}});
+          for (int w : {1, 2}) cands.push_back(mccfr_batch_tuning{blk, grab, k, w, ws, MCCFR_BATCH_PERSISTENT, {0, 0}});
   if (max_candidates > 0 && (int)cands.size() > max_candidates) cands.resize(max_candidates);
   // Candidates run on successive real iterations, whose trees change as the
   // strategy sharpens; each is ranked by traversal-kernel time per node visit,
@@ -2320,7 +2379,7 @@ int mccfr_get_progress(mccfr_handle* h, long long* next_iteration, int* next_pla
 
 int mccfr_batch_round(mccfr_handle* const* tables, int n, const int* traversals, const mccfr_batch_tuning* tuning) {
   if (!tables || !traversals || n < 1 || n > kMaxBatchTables) return MCCFR_ERR_INVALID_ARG;
-  mccfr_batch_tuning t{128, 1, 0, 1, 1, {0, 0, 0}};
+  mccfr_batch_tuning t{128, 1, 0, 1, 1, MCCFR_BATCH_PERSISTENT, {0, 0}};
   if (tuning) {
     if (!valid_tuning(*tuning)) return MCCFR_ERR_INVALID_ARG;
     t = *tuning;

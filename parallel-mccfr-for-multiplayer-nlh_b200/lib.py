@@ -34,6 +34,7 @@ PREFLOP_CHEN64, PREFLOP_CLASS169 = 0, 1
 POSTFLOP_REF_LINEAR, POSTFLOP_RANK_CDF = 0, 1
 PRESET_REF8, PRESET_HU_20BB, PRESET_6MAX_100BB = 0, 1, 2
 FORM_AUTO, FORM_LANES, FORM_LEVELS = 0, 1, 2
+BATCH_PERSISTENT, BATCH_TABLE_GRAPHS = 0, 1
 
 
 class Config(Structure):
@@ -70,11 +71,11 @@ class Stats(Structure):
 
 class BatchTuning(Structure):
     _fields_ = [("block", c_int32), ("grab", c_int32), ("smem_frames", c_int32), ("probe_width", c_int32),
-                ("warp_sync", c_int32), ("reserved", c_int32 * 3)]
+                ("warp_sync", c_int32), ("form", c_int32), ("reserved", c_int32 * 2)]
 
     def as_dict(self) -> dict:
         return {"block": self.block, "grab": self.grab, "smem_frames": self.smem_frames,
-                "probe_width": self.probe_width, "warp_sync": self.warp_sync}
+                "probe_width": self.probe_width, "warp_sync": self.warp_sync, "form": self.form}
 
 
 class BatchStats(Structure):

@@ -298,12 +298,15 @@ class Batch:
 
     @staticmethod
     def candidates(max_candidates: int = 0) -> list:
-        c = [dict(block=b, grab=g, smem_frames=k, probe_width=w, warp_sync=s)
+        c = [dict(block=b, grab=g, smem_frames=k, probe_width=w, warp_sync=s, form=L.BATCH_PERSISTENT)
              for b in (128, 64, 256) for g in (1, 2, 4, 8) for k in (0, 2, 4) for s in (1, 0) for w in (1, 2)]
         return c[:max_candidates] if max_candidates > 0 else c
 
-    def set_tuning(self, block=128, grab=2, smem_frames=0, probe_width=1, warp_sync=1) -> None:
-        t = L.BatchTuning(block, grab, smem_frames, probe_width, warp_sync)
+    def set_tuning(self, block=128, grab=2, smem_frames=0, probe_width=1, warp_sync=1, form=0) -> None:
+        """form: L.BATCH_PERSISTENT (one persistent traversal launch per phase
+        over all tables, tuned by the other fields) or L.BATCH_TABLE_GRAPHS (each
+        table's own update kernels as concurrent branches of one graph)."""
+        t = L.BatchTuning(block, grab, smem_frames, probe_width, warp_sync, form)
         L.check(self._lib.mccfr_batch_set_tuning(self._b, byref(t)))
 
     def tuning(self) -> dict:

@@ -1,5 +1,7 @@
-"""The batched persistent form against the plain trainer: every table of a
-batch ends bit-identical to the same table trained alone, whatever the tuning."""
+"""The batched forms against the plain trainer: every table of a batch ends
+bit-identical to the same table trained alone, whatever the tuning and form
+(one persistent traversal launch per phase, or every table's own update
+kernels as concurrent branches of one graph)."""
 from __future__ import annotations
 
 import numpy as np
@@ -72,4 +74,29 @@ def test_autotune_keeps_results(hand_table):
         t.train(13, n, verbose=False)
     for p, q in zip(plain, batched):
         rows_equal(p.export_rows(), q.export_rows())
+    b.close()
+
+
+def test_table_graph_form_equals_plain(hand_table):
+    """Two iterations in the table-graph form, then one in the persistent form and
+    one more in the table-graph form: each table equals four iterations of
+    training it alone (the level-synchronous kernels in its branch)."""
+    cfgs, trav = small_tables()
+    plain = make(cfgs, hand_table)
+    for t, n in zip(plain, trav):
+        t.train(4, n, verbose=False)
+    batched = make(cfgs, hand_table)
+    b = mccfr.Batch(batched, trav)
+    b.set_tuning(form=L.BATCH_TABLE_GRAPHS)
+    b.train(2, timed=True)
+    b.set_tuning(form=L.BATCH_PERSISTENT)
+    b.train(1)
+    b.set_tuning(form=L.BATCH_TABLE_GRAPHS)
+    b.train(1)
+    for p, q in zip(plain, batched):
+        rows_equal(p.export_rows(), q.export_rows())
+    st = b.stats()
+    assert st.iterations == 4
+    assert st.traversals == sum(4 * n * c.num_players for n, c in zip(trav, cfgs))
+    assert st.total_ms > 0
     b.close()
