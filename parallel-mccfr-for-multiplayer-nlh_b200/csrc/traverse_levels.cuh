@@ -11,13 +11,17 @@
 //              opponents' nodes (each samples one action and adds its strategy
 //              to the row's strategy sum, as in the depth-first walk), street
 //              changes and terminals, until it reaches a terminal (the seed's
-//              value) or an updating-player node.  That node gets a record (its
-//              state, row slot, legal mask) and every legal action becomes a
-//              seed of level L+1.  Lanes take seeds from a per-level counter as
-//              they finish, so a warp keeps its lanes busy whatever the walks'
-//              lengths.
+//              value; a showdown leaves a record for the showdown pass) or an
+//              updating-player node.  That node gets a record (its state, row
+//              slot, legal mask) and every legal action becomes a seed of level
+//              L+1.  Warps take seeds 32 at a time from a per-level counter and
+//              hand them to idle lanes as those finish, so a warp keeps its
+//              lanes busy whatever the walks' lengths.
 //   dfs        seeds that did not fit the buffers (see below) are walked depth
 //              first by the frame-stack walk of k_traverse_es, from the seed.
+//   showdown   the recorded showdowns' side-pot payoffs, one thread each, so
+//              that the walk's loop never runs the side-pot arithmetic for a
+//              few of its lanes.
 //   back(L)    one thread per updating-player node of level L, deepest level
 //              first: it regret-matches the node's row (its regrets are a
 //              snapshot the update does not change), reads its children's values,
@@ -33,12 +37,14 @@
 // bit-identical to the depth-first walk's, whatever the order of the lanes.
 //
 // Buffers.  A level's updating-player nodes and child seeds are appended to
-// two bump-allocated arrays (nodes: 64 B state + 16 B record; seeds: 8 B).  A
+// two bump-allocated arrays (nodes: 64 B state + 16 B record; seeds: 8 B),
+// both by one 64-bit add per warp step ((nodes << 32) | seeds).  A
 // lane checks, when it picks a seed up, that the arrays still have room for
 // the worst case of every lane that may hold a seed meanwhile (one node and
 // num_actions seeds each); a seed that fails the check is marked and left to
-// the dfs kernel, unwalked.  So no allocation can overflow, and any buffer size
-// gives the same rows.
+// the dfs kernel, unwalked.  A showdown past the end of its record list is
+// evaluated by the lane that reached it.  So no allocation can overflow, and
+// any buffer size gives the same rows.
 #pragma once
 #include "game.cuh"
 #include "table.cuh"
