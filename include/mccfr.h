@@ -324,8 +324,8 @@ int mccfr_showdown_masks(mccfr_handle* h, long long iteration, int player, size_
    player-p updates of every table with more than p players, pulling
    traversals from a device work queue, then one apply launch for those tables.
    Each table's result is bit-identical to training it alone with the same
-   traversals per update.  All handles must be on one device, hold a rank
-   table, use external sampling, and not be used elsewhere while batched. */
+   traversals per update.  All handles must be distinct, on one device, hold a
+   rank table, use external sampling, and not be used elsewhere while batched. */
 typedef struct mccfr_batch mccfr_batch;
 typedef struct mccfr_batch_tuning {
   int32_t block;          /* threads per block: 64, 128 or 256 */

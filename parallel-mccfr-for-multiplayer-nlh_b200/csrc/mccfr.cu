@@ -1969,6 +1969,8 @@ int mccfr_batch_create(mccfr_handle* const* tables, int n, const int* traversals
     if (h->device != b->device) return bad(MCCFR_ERR_INVALID_ARG, "tables on different devices");
     if (!h->has_table) return bad(MCCFR_ERR_NO_HAND_TABLE, "a table has no rank table loaded");
     if (h->cfg.sampling != MCCFR_SAMPLING_EXTERNAL) return bad(MCCFR_ERR_INVALID_ARG, "batched tables use external sampling");
+    for (mccfr_handle* o : b->tables)
+      if (o == h) return bad(MCCFR_ERR_INVALID_ARG, "a table appears twice in the batch");
     b->tables.push_back(h);
     b->traversals.push_back(traversals[i]);
     b->max_players = std::max(b->max_players, h->cfg.num_players);
