@@ -259,8 +259,9 @@ class GPUCFRTrainer:
 
 
 class Batch:
-    """Several trainers (tables) trained together by one persistent kernel per
-    phase; each table's result equals training it alone (mccfr_batch_*)."""
+    """Several trainers (tables) trained together, by one persistent kernel per
+    phase or as concurrent branches of one graph (set_tuning(form=...)); each
+    table's result equals training it alone (mccfr_batch_*)."""
 
     def __init__(self, trainers: list, traversals: list[int]):
         self._lib = L.load()

@@ -100,3 +100,11 @@ def test_table_graph_form_equals_plain(hand_table):
     assert st.traversals == sum(4 * n * c.num_players for n, c in zip(trav, cfgs))
     assert st.total_ms > 0
     b.close()
+
+
+def test_a_table_twice_is_refused(hand_table):
+    cfgs, trav = small_tables()
+    ts = make(cfgs[:1], hand_table)
+    with pytest.raises(L.MccfrError):
+        mccfr.Batch([ts[0], ts[0]], [trav[0], trav[0]])
+    ts[0].close()
