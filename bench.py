@@ -296,7 +296,7 @@ def reference_arm(args, workload: str, world: int) -> dict:
         "impl": "reference", "metric": metric, "value": v, "unit": "traversals/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / max(1, args.steps),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": describe(cfg, workload, batch),
+        "config": {**describe(cfg, workload, batch), "parallelism": f"replicas{world}"},
         "cpu_baseline": {"value": v, "unit": "traversals/s", "cores": threads, "kind": "port", "sample": sample,
                          "V_per_traversal": vpt, "U_per_traversal": upt, "traversals_per_update": b},
         "e2e": {"value": v, "unit": "traversals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
