@@ -360,12 +360,16 @@ int mccfr_batch_create(mccfr_handle* const* tables, int n_tables, const int* tra
 void mccfr_batch_destroy(mccfr_batch* b);
 int mccfr_batch_set_tuning(mccfr_batch* b, const mccfr_batch_tuning* t);
 int mccfr_batch_get_tuning(mccfr_batch* b, mccfr_batch_tuning* t);
-/* Runs `iters` iterations of every table (one CUDA graph per iteration).
+/* Runs `iters` iterations of every table (one CUDA graph per iteration), in the
+   form of the batch's tuning: a new batch runs MCCFR_BATCH_TABLE_GRAPHS until
+   mccfr_batch_set_tuning or mccfr_batch_autotune (which tunes the persistent
+   form) changes it.
    flags bit 1: time every iteration with CUDA events (synchronises per iteration). */
 int mccfr_batch_train(mccfr_batch* b, long long iters, int flags);
 /* Trains two real iterations per candidate tuning, the list forward then
    backward (results do not depend on the tuning), and keeps the candidate with
-   the least summed traversal-kernel time per node visit; *best receives it.
+   the least summed traversal-kernel time per node visit; *best receives it and
+   becomes the batch's tuning (persistent form).
    Candidates: block x grab x smem_frames x warp_sync x probe_width from the
    sets above, limited to the first `max_candidates` (0 = all 144). */
 int mccfr_batch_autotune(mccfr_batch* b, int max_candidates, mccfr_batch_tuning* best);

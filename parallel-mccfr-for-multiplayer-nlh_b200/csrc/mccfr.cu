@@ -1781,7 +1781,7 @@ struct mccfr_batch {
   DealRec* d_deals = nullptr;
   unsigned long long* d_work = nullptr;
   unsigned long long max_items = 0;
-  mccfr_batch_tuning tuning{128, 2, 0, 1, 1, MCCFR_BATCH_PERSISTENT, {0, 0}};
+  mccfr_batch_tuning tuning{128, 2, 0, 1, 1, MCCFR_BATCH_TABLE_GRAPHS, {0, 0}};  // until set or autotuned
   cudaGraphExec_t graph = nullptr;
   cudaEvent_t ev_fork = nullptr;       // table-graph form: fork and joins of the tables' branches
   std::vector<cudaEvent_t> ev_join;
