@@ -100,11 +100,11 @@ def test_level_buffers_smaller_than_the_update(hand_table, lg):
     """The level form with node buffers far below its default of 64 per
     traversal (2^lg node records for 4,096 traversals, and as many showdown
     records): a seed that may not fit is left to the depth-first kernel (at
-    lg = 8 every root is, at lg = 14 the levels below the first), and a showdown
-    past the end of its record list is evaluated where it is reached (at
-    iteration 1 a traversal reaches more showdowns than lg = 16 leaves records
-    for).  Three iterations from an empty table; the table digest equals the
-    oracle's after each, and every row after the last."""
+    lg = 8 every root is, at lg = 14 the levels below the first, at lg = 16
+    whatever no longer fits part-way through a level), and a showdown past the
+    end of its record list is evaluated where it is reached.  Three iterations
+    from an empty table; the table digest equals the oracle's after each, and
+    every row after the last."""
     cfg = L.preset(L.PRESET_6MAX_100BB)
     cfg.table_log2, cfg.key_bits = 22, 21
     cfg.traversal_form = L.FORM_LEVELS
